@@ -1,0 +1,287 @@
+"""Benchmark: batched river CFR+ solves/s on one or more B200s.
+
+Workload: the batched uneven river configuration — 4,096 seeded subgames per
+GPU (1-4 bet sizes from 25-200% pot, raise cap 1-3, range supports of 200-1,081
+combos with lognormal(0,1) weights, pot 20-200, SPR 0.5-12), 1,000 CFR+
+iterations each in FP32, then the FP64 best-response exploitability pass.
+One step = one solve of the whole batch.  Each GPU solves its own batch
+(weak scaling, replicas only: no data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed with inputs resident
+in HBM; `e2e` goes through the public C ABI from host buffers (pack + H2D +
+solve + D2H of the results) per step.
+"""
+import argparse
+import concurrent.futures
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "batched river solves/s at <=0.1% pot exploitability vs plain kernel; evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--subgames", type=int, default=4096)
+    ap.add_argument("--iters", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=0, help="subgames in the CPU baseline sample (0 = auto)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_solves_per_s(subs, iters, n_sample, budget_s=20.0):
+    """The CPU restatement of the reference sweeps (oracle), all host cores,
+    on a bounded sample: n_sample subgames for a fraction of the iterations,
+    scaled to full solves (the per-iteration cost does not depend on t)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    pyoracle.lib()
+    cores = os.cpu_count() or 1
+    sample = subs[:n_sample]
+    # calibrate: one iteration of the sample, then size the run to the budget
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(lambda g: pyoracle.cfr_solve(g, 1), sample))
+    t1 = time.perf_counter() - t0
+    it = int(max(1, min(iters, budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(lambda g: pyoracle.cfr_solve(g, it), sample))
+    el = time.perf_counter() - t0
+    per_solve = el / len(sample) * (iters / it)
+    return 1.0 / per_solve, cores, f"{len(sample)} of the subgames x {it} of {iters} CFR+ iterations, " \
+        f"dense O(H^2) showdowns, {cores} threads; scaled to full solves"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    wl = importlib.import_module("mtt-gpu-solver_b200.workloads")
+    subs = wl.river_batch(n=args.subgames, seed=args.seed)
+    n_sample = args.cpu_sample or max(os.cpu_count() or 1, 8)
+    vals = []
+    cores, sample = 1, ""
+    for _ in range(args.warmup + args.steps):
+        v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, n_sample, budget_s=5.0)
+        vals.append(v)
+    v = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.subgames / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames x {args.iters} iters",
+                       "subgames": args.subgames, "iters": args.iters, "seed": args.seed},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    mtt = importlib.import_module("mtt-gpu-solver_b200")
+    wl = importlib.import_module("mtt-gpu-solver_b200.workloads")
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    subs = wl.river_batch(n=args.subgames, seed=args.seed + 1000 * rank)
+    p = mtt.solve_params(iters=args.iters, threads=0, exploitability=True)
+    stream = torch.cuda.current_stream()
+    batch = mtt.RiverBatch(subs)
+    threads = batch.autotune(p)
+    p.threads = threads
+    info = batch.info()
+
+    def step():
+        batch.solve(p, graph=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    res = batch.results()
+    expl = res[:, 5]
+    # dominant kernel alone (no best response): algorithmic bytes / event time
+    ps = mtt.solve_params(iters=args.iters, threads=threads, exploitability=False)
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    batch.solve(ps)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    solve_ms = k0.elapsed_time(k1)
+    algo_bytes = info["iter_bytes"] * args.iters
+    achieved = algo_bytes / (solve_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+    batch.close()
+
+    # end to end through the public API from host buffers
+    def e2e_step():
+        b = mtt.RiverBatch(subs)
+        b.solve(p)
+        r = b.results()
+        b.close()
+        return r
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 2))):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
+    if pg:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(g["nodes"].nbytes + g["combos0"].nbytes + g["combos1"].nbytes + g["range0"].nbytes +
+              g["range1"].nbytes for g in subs)
+
+    # evaluator throughput (all C(52,7) hands)
+    mtt.eval7_enumerate()
+    torch.cuda.synchronize()
+    v0 = torch.cuda.Event(enable_timing=True)
+    v1 = torch.cuda.Event(enable_timing=True)
+    v0.record(stream)
+    for _ in range(5):
+        mtt.eval7_enumerate()
+    v1.record(stream)
+    torch.cuda.synchronize()
+    evals_per_s = 5 * 133784560 / (v0.elapsed_time(v1) * 1e-3)
+
+    value = args.subgames * world / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
+            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames x {args.iters} iters "
+                                   f"+ FP64 exploitability", "subgames_per_gpu": args.subgames,
+                       "iters": args.iters, "seed": args.seed, "cta_threads": threads,
+                       "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (info["device_bytes"] / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "exploitability_pct_pot": {"median": float(np.median(expl) * 100), "max": float(np.max(expl) * 100),
+                                       "frac_le_0.1pct": float(np.mean(expl <= 1e-3))},
+            "evals_per_s": evals_per_s,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_batch_solve",
+                         "peak_kind": peak_kind, "kernel_ms": solve_ms},
+            "clocks": clocks,
+            "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(args.subgames * 6 * 8)},
+            "gpu_launches": 2 * args.steps}
+    if rank == 0 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, args.cpu_sample or max(os.cpu_count() or 1, 8))
+        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

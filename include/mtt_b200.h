@@ -1,0 +1,229 @@
+/*
+ * mtt_b200.h — C ABI of the B200 (sm_100a) hot path of MTT-GPU-Solver.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (MTT_OK == 0) and never exits the process.  Unless stated otherwise,
+ * pointers whose name starts with d_ are device pointers owned by the caller,
+ * h_ pointers are host pointers, and `stream` is a cudaStream_t passed as
+ * void* (NULL = the legacy default stream).  Calls on different devices or
+ * different streams may run concurrently from different host threads; a
+ * handle (mtt_solver / mtt_batch) is used by one host thread at a time.
+ *
+ * Card encoding follows the reference: card = rank*4 + suit, rank 0='2' ..
+ * 12='A', suit 0..3 = c,d,h,s (src/tools/mtt_ev_dumper.cu:27,
+ * scripts/optimize_subset.py:59-61).  A hole-card combo is an unordered pair
+ * (c1 < c2); combo ids 0..1325 enumerate the pairs lexicographically.
+ *
+ * Reference citations are file:line inside the MTT-GPU-Solver project.
+ */
+#ifndef MTT_B200_H
+#define MTT_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; everything declared here is exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define MTT_OK              0
+#define MTT_ERR_INVALID     1   /* bad argument, size or tree */
+#define MTT_ERR_CUDA        2   /* a CUDA runtime call failed (see mtt_last_cuda_error) */
+#define MTT_ERR_NOMEM       3   /* device or host allocation failed */
+#define MTT_ERR_TIMEOUT     4   /* a bounded device wait gave up */
+#define MTT_ERR_IO          5   /* file missing, short or malformed */
+#define MTT_ERR_UNSUPPORTED 6   /* size or feature outside what this build handles */
+
+/* Human-readable name of a status code (static string). */
+const char* mtt_status_string(int status);
+/* cudaError_t value of the last failing CUDA call on this host thread (0 if none). */
+int mtt_last_cuda_error(void);
+/* Library version string. */
+const char* mtt_version(void);
+
+/* ------------------------------------------------------------- game trees */
+#define MTT_NODE_DECISION 0
+#define MTT_NODE_FOLD     1
+#define MTT_NODE_SHOWDOWN 2
+#define MTT_NODE_CHANCE   3
+
+/* Flat heads-up tree node, 32 bytes.  The field order, widths and meaning
+ * follow the reference's FlatNode (src/postflop/honest_multistreet_solver.cu:14-21):
+ * children are contiguous at children_offset + a; a fold node's active_mask
+ * has the bit of the player who did NOT fold; pot_size and committed[] are
+ * chips, and each player's committed[] includes half of the starting pot, so
+ * payoffs are zero-sum.  Two differences, both in fields the reference leaves
+ * implicit: infoset_offset is the first row of this node in ITS PLAYER's own
+ * regret array (rows are numbered per player, one row per action, so the
+ * reference's info*MAX_ACTIONS+a becomes infoset_offset+a), and the 2-byte
+ * pad after turn_idx holds the node depth.  turn_idx is the card dealt by the
+ * parent chance node (-1 when there is none). */
+typedef struct mtt_node {
+    uint8_t  type;
+    uint8_t  player;
+    uint8_t  num_actions;
+    uint8_t  active_mask;
+    int32_t  children_offset;
+    int32_t  infoset_offset;
+    int16_t  turn_idx;
+    int16_t  depth;
+    float    pot_size;
+    float    committed[2];
+    float    reserved;
+} mtt_node;
+
+#define MTT_MAX_SIZES 8
+/* Betting abstraction for one heads-up subgame.  Sizes are fractions of the
+ * pot; a raise size f puts in to_call + f*(pot + to_call).  Any size at or
+ * above the remaining stack becomes all-in.  raise_cap counts raises after
+ * the first bet of a street. street = 5: river subgame (5-card board);
+ * street = 4: turn subgame whose betting rounds close into a river chance
+ * node (48 children) followed by a river subgame with the same sizes. */
+typedef struct mtt_tree_spec {
+    float   pot;
+    float   stack;
+    int32_t n_bet_sizes;
+    float   bet_sizes[MTT_MAX_SIZES];
+    int32_t n_raise_sizes;              /* 0: raises reuse bet_sizes */
+    float   raise_sizes[MTT_MAX_SIZES];
+    int32_t raise_cap;
+    int32_t allin;                      /* 1: all-in is always offered */
+    int32_t street;                     /* 5 or 4 */
+} mtt_tree_spec;
+
+/* Build the tree in breadth-first order (children contiguous, parents first).
+ * nodes may be NULL to query the size.  Outputs: *n_nodes, rows per player
+ * (rows[2]: regret rows of player 0 and 1), *max_depth. Host only. */
+int mtt_tree_build(const mtt_tree_spec* spec, mtt_node* nodes, int32_t capacity,
+                   int32_t* n_nodes, int32_t rows[2], int32_t* max_depth);
+
+/* Turn subgame (spec->street == 4, board = 4 cards): every betting round that
+ * closes with chips behind goes to a river chance node with one child per
+ * card not on the board, followed by a river round; all-in calls go to a
+ * chance node whose children are showdowns.  Also accepts street == 5 with a
+ * 5-card board.  Host only. */
+int mtt_tree_build_board(const mtt_tree_spec* spec, const uint8_t* board, int32_t nboard,
+                         mtt_node* nodes, int32_t capacity, int32_t* n_nodes, int32_t rows[2],
+                         int32_t* max_depth);
+
+/* Check a caller-supplied tree (reference FlatNode layout, rows per player as
+ * above): offsets in range, children after parents, actions >= 1, no cycles.
+ * Host only. */
+int mtt_tree_validate(const mtt_node* nodes, int32_t n_nodes, int32_t rows[2]);
+
+/* ------------------------------------------------------------- evaluator */
+/* 7 cards per hand (uint8 x 7, packed) -> uint32 score identical to the
+ * reference's fast_7card_score (src/tools/mtt_ev_dumper.cu:53-83; copies at
+ * honest_multistreet_solver.cu:24-54 and preflop_grid_generator.cu:47-77). */
+int mtt_eval7(const uint8_t* d_cards7, uint32_t* d_out, int64_t n, void* stream);
+
+/* Evaluate all C(52,7) hands: d_hist9[k] = hands of category k (score>>24),
+ * *d_checksum = sum over hands in colex order of score*(index+1) mod 2^64.
+ * If d_key_table (65,536 uint32) is given it receives key -> score for the
+ * 16-bit monotone key the scans use; *d_err gets bit 1 if two scores share a
+ * key.  Replaces the survey-style full enumeration of the reference scorer. */
+int mtt_eval7_enumerate(uint64_t* d_hist9, uint64_t* d_checksum, uint32_t* d_key_table,
+                        int32_t* d_err, void* stream);
+
+/* ------------------------------------------------------ showdown counts */
+/* Exact win/tie/loss counts of hero i vs villain j (out[i*H+j], int32) over
+ * every completion of a 3-, 4- or 5-card board.  Pairs that share a card or
+ * touch the board get zeros.  Replaces kernel_gen_49_turn_matrices
+ * (src/postflop/honest_multistreet_solver.cu:56-86), whose float entry is
+ * (W + 0.5*T) / (W + T + L) of these counts; its output is villain-major,
+ * this one hero-major. */
+int mtt_board_showdown_counts(const uint8_t* d_board, int32_t nboard, const uint8_t* d_hands,
+                              int32_t H, int32_t* d_w, int32_t* d_t, int32_t* d_l, void* stream);
+
+/* ------------------------------------------------------------ dumper path */
+/* The 1,755 canonical flops with orbit weights, h_out[4*i..] = c1,c2,c3,w
+ * (generate_all_1755_flops, src/tools/mtt_ev_dumper.cu:34-51). Host only. */
+int mtt_canonical_flops(uint8_t* h_out, int32_t capacity, int32_t* n_out);
+
+/* kernel_evaluate_flop_ev (src/tools/mtt_ev_dumper.cu:85-116) for nflops flops
+ * (d_flops: 3 cards each).  d_reach0/1: 1,176 weights over the flop's alive
+ * combos in lexicographic order (NULL = uniform 1/1176).  d_ev0/1: [nflops][1176].
+ * Bit-exact with the reference. */
+int mtt_flop_ev(const uint8_t* d_flops, int32_t nflops, const float* d_reach0,
+                const float* d_reach1, float* d_ev0, float* d_ev1, void* stream);
+
+/* ev_dumper's output for nflops flops: d_out [nflops][4][2][169] f32, the
+ * per-flop slices of mtt_ev_dump_1755.bin (mtt_ev_dumper.cu:141-173).
+ * Bit-exact with the reference's shipped file. */
+int mtt_ev_dump(const uint8_t* d_flops, int32_t nflops, float* d_out, void* stream);
+
+/* --------------------------------------------------- heads-up CFR solving */
+#define MTT_ALGO_CFRPLUS 0     /* R <- max(0, R + r); S += t * reach * sigma */
+#define MTT_ALGO_DCFR    1     /* discount R (alpha/beta) and S (gamma), then add */
+#define MTT_SEM_CORRECT   0    /* card removal at showdown and fold, ties split, chance / (N-4) */
+#define MTT_SEM_REFERENCE 1    /* the reference kernels' semantics: P1 showdown equity inverted,
+                                  no card removal between the hands, chance / (N-2)
+                                  (honest_multistreet_solver.cu:163-164,182-187,217) */
+
+typedef struct mtt_solve_params {
+    int32_t iters;
+    int32_t algo;
+    float   alpha, beta, gamma;   /* DCFR only */
+    int32_t semantics;
+    int32_t threads;              /* CTA size of the batched kernel (64/128/256); 0 = autotuned */
+    int32_t exploitability;       /* 1: FP64 best-response pass after the iterations */
+} mtt_solve_params;
+
+/* One heads-up subgame.  combos[p] ascending combo ids (0..1325) of player
+ * p's range support, none touching the board; ranges[p] their weights. */
+typedef struct mtt_subgame {
+    const mtt_node* nodes;
+    int32_t n_nodes;
+    int32_t rows[2];
+    uint8_t board[5];
+    int32_t nboard;               /* 5 river, 4 turn (tree has river chance nodes) */
+    int32_t H[2];
+    const uint16_t* combos[2];
+    const float* ranges[2];
+} mtt_subgame;
+
+typedef struct mtt_batch mtt_batch;
+
+/* Pack n subgames (host pointers) into device memory on the current device.
+ * Synchronous.  Per subgame the layout is reach/CFV vectors per node, R and S
+ * per regret row, and per-board showdown rank tables. */
+int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** out);
+/* Solve every subgame from zero regrets: one persistent kernel, one CTA per
+ * subgame at a time from a work queue (largest first), then (optionally) the
+ * FP64 best-response kernel.  Asynchronous on stream. */
+int mtt_batch_solve(mtt_batch* b, const mtt_solve_params* prm, void* stream);
+/* Same work as mtt_batch_solve, replayed from a CUDA graph captured on the
+ * first call for these params. */
+int mtt_batch_solve_graph(mtt_batch* b, const mtt_solve_params* prm, void* stream);
+/* Per subgame: [0] BR value of P0, [1] BR of P1, [2] EV of P0 under the
+ * average strategies, [3] EV of P1 (per unit of compatible range mass),
+ * [4] compatible range mass Z, [5] exploitability (BR0+BR1)/2 / starting pot.
+ * Waits for the stream. */
+int mtt_batch_results(mtt_batch* b, double* h_out, void* stream);
+/* Regrets R_p, strategy sums S_p ([rows_p][H_p]) and last-iteration root
+ * CFVs (cfv_p[H_p]) of subgame s; any pointer may be NULL.  Synchronous. */
+int mtt_batch_read(mtt_batch* b, int32_t s, float* h_R0, float* h_R1, float* h_S0, float* h_S1,
+                   float* h_cfv0, float* h_cfv1);
+/* Device bytes held, and algorithmic bytes of one CFR iteration over the whole
+ * batch (R,S read+write per action-hand; reach and CFV written and read once
+ * per player-hand per node). */
+int mtt_batch_info(mtt_batch* b, int64_t* device_bytes, int64_t* iter_bytes);
+/* Pick the CTA size by timing a few iterations of each candidate on this
+ * batch; *threads receives the choice (also used when params.threads == 0). */
+int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads);
+int mtt_batch_destroy(mtt_batch* b);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MTT_B200_H */

@@ -1,0 +1,106 @@
+"""ctypes binding of libmtt_b200.so (the C ABI declared in include/mtt_b200.h).
+
+The shared library is built in-tree by build.py; importing this module loads
+it and fails loudly if it is missing.  There is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmtt_b200.so")
+
+MTT_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "timeout", 5: "io",
+          6: "unsupported"}
+
+NODE_DECISION, NODE_FOLD, NODE_SHOWDOWN, NODE_CHANCE = 0, 1, 2, 3
+ALGO_CFRPLUS, ALGO_DCFR = 0, 1
+SEM_CORRECT, SEM_REFERENCE = 0, 1
+
+# mtt_node: the reference FlatNode layout (honest_multistreet_solver.cu:16-21), 32 bytes
+NODE_DTYPE = np.dtype([
+    ("type", "u1"), ("player", "u1"), ("num_actions", "u1"), ("active_mask", "u1"),
+    ("children_offset", "<i4"), ("infoset_offset", "<i4"), ("turn_idx", "<i2"), ("depth", "<i2"),
+    ("pot_size", "<f4"), ("committed", "<f4", (2,)), ("reserved", "<f4"),
+])
+assert NODE_DTYPE.itemsize == 32
+
+
+class TreeSpec(ctypes.Structure):
+    _fields_ = [("pot", ctypes.c_float), ("stack", ctypes.c_float),
+                ("n_bet_sizes", ctypes.c_int32), ("bet_sizes", ctypes.c_float * 8),
+                ("n_raise_sizes", ctypes.c_int32), ("raise_sizes", ctypes.c_float * 8),
+                ("raise_cap", ctypes.c_int32), ("allin", ctypes.c_int32), ("street", ctypes.c_int32)]
+
+
+class SolveParams(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("algo", ctypes.c_int32), ("alpha", ctypes.c_float),
+                ("beta", ctypes.c_float), ("gamma", ctypes.c_float), ("semantics", ctypes.c_int32),
+                ("threads", ctypes.c_int32), ("exploitability", ctypes.c_int32)]
+
+
+class Subgame(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int32), ("rows", ctypes.c_int32 * 2),
+                ("board", ctypes.c_uint8 * 5), ("nboard", ctypes.c_int32), ("H", ctypes.c_int32 * 2),
+                ("combos", ctypes.c_void_p * 2), ("ranges", ctypes.c_void_p * 2)]
+
+
+class MttError(RuntimeError):
+    def __init__(self, fn, status, cuda_err=0):
+        super().__init__(f"{fn} failed: {STATUS.get(status, status)} (status {status}, cudaError {cuda_err})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with python mtt-gpu-solver_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    sig = {
+        "mtt_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "mtt_last_cuda_error": ([], ctypes.c_int),
+        "mtt_version": ([], ctypes.c_char_p),
+        "mtt_tree_build": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_tree_build_board": ([vp, vp, i32, vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_tree_validate": ([vp, i32, vp], ctypes.c_int),
+        "mtt_eval7": ([vp, vp, i64, vp], ctypes.c_int),
+        "mtt_eval7_enumerate": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_board_showdown_counts": ([vp, i32, vp, i32, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_canonical_flops": ([vp, i32, vp], ctypes.c_int),
+        "mtt_flop_ev": ([vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_ev_dump": ([vp, i32, vp, vp], ctypes.c_int),
+        "mtt_batch_create": ([vp, i32, vp], ctypes.c_int),
+        "mtt_batch_solve": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_solve_graph": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_results": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_read": ([vp, i32, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_info": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_autotune": ([vp, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_destroy": ([vp], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(fn, status):
+    if status != MTT_OK:
+        raise MttError(fn, status, lib().mtt_last_cuda_error())
+
+
+def exported_symbols():
+    """Names of the functions include/mtt_b200.h declares."""
+    import re
+    hdr = open(os.path.join(os.path.dirname(HERE), "include", "mtt_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(mtt_[a-z0-9_]+)\s*\(", hdr, re.M)))

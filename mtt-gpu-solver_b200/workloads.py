@@ -1,0 +1,69 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+No public dataset is involved: boards, ranges and betting abstractions are
+drawn from numpy's PCG64 generator with a fixed seed.
+
+* river_uniform (config 0): one HU river subgame, 5-card board from the seed,
+  both ranges uniform over the 1,081 board-compatible combos, pot 100, stack
+  200, bets {50%, 100%} + all-in, one raise.
+* river_batch (config 2): n uneven river subgames; per subgame 1-4 bet sizes
+  from U[25%, 200%], raise cap 1-3, supports of 200-1,081 combos with
+  lognormal(0, 1) weights, pot U[20, 200], SPR U[0.5, 12].
+"""
+import numpy as np
+
+from . import build_tree, live_combos
+
+
+def draw_board(rng, n=5):
+    return [int(c) for c in rng.choice(52, size=n, replace=False)]
+
+
+def _tree_cached(cache, pot, stack, sizes, cap, street=5, board=None):
+    key = (round(float(pot), 6), round(float(stack), 6), tuple(round(float(s), 6) for s in sizes), int(cap), street,
+           tuple(board) if board is not None else None)
+    t = cache.get(key)
+    if t is None:
+        t = build_tree(pot, stack, list(sizes), raise_cap=cap, street=street, board=board)
+        cache[key] = t
+    return t
+
+
+def river_uniform(seed=0, pot=100.0, stack=200.0, bet_sizes=(0.5, 1.0), raise_cap=1, n_hands=None):
+    """Config 0.  n_hands (optional) restricts both ranges to the first
+    n_hands live combos (small parity cases)."""
+    rng = np.random.default_rng(seed)
+    board = draw_board(rng)
+    live = live_combos(board)
+    if n_hands is not None:
+        live = np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
+    nodes, rows, _ = build_tree(pot, stack, list(bet_sizes), raise_cap=raise_cap)
+    r = np.full(len(live), 1.0 / len(live), dtype=np.float32)
+    return {"nodes": nodes, "rows": rows, "board": board, "combos0": live, "combos1": live.copy(),
+            "range0": r, "range1": r.copy(), "pot": pot}
+
+
+def river_batch(n=4096, seed=2, min_support=200, max_support=1081, max_sizes=4):
+    """Config 2 (the batched uneven river workload)."""
+    rng = np.random.default_rng(seed)
+    cache = {}
+    subs = []
+    for _ in range(n):
+        board = draw_board(rng)
+        live = live_combos(board)
+        nsz = int(rng.integers(1, max_sizes + 1))
+        sizes = np.sort(rng.uniform(0.25, 2.0, size=nsz)).round(3)
+        cap = int(rng.integers(1, 4))
+        pot = float(np.round(rng.uniform(20.0, 200.0), 1))
+        spr = float(np.round(rng.uniform(0.5, 12.0), 2))
+        stack = float(np.round(pot * spr, 1))
+        nodes, rows, _ = _tree_cached(cache, pot, stack, sizes, cap)
+        g = {"nodes": nodes, "rows": rows, "board": board, "pot": pot}
+        for p in (0, 1):
+            k = int(rng.integers(min_support, min(max_support, len(live)) + 1))
+            sup = np.sort(rng.choice(live, size=k, replace=False)).astype(np.uint16)
+            w = rng.lognormal(0.0, 1.0, size=k).astype(np.float32)
+            g[f"combos{p}"] = sup
+            g[f"range{p}"] = w
+        subs.append(g)
+    return subs

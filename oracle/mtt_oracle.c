@@ -1,0 +1,674 @@
+/*
+ * mtt_oracle.c — CPU oracle (TEST INFRASTRUCTURE ONLY; see mtt_oracle.h).
+ *
+ * Plain-C restatement of the reference kernels of MTT-GPU-Solver.  Each
+ * function cites the reference lines it follows.  Built with
+ * -ffp-contract=off so that the only fused multiply-adds are the explicit
+ * fmaf() calls standing in for the contractions nvcc makes in the reference
+ * kernels; divisions are IEEE.
+ */
+#include "mtt_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Evaluator: restates fast_7card_score (src/tools/mtt_ev_dumper.cu:53-83),  */
+/* identical copies at honest_multistreet_solver.cu:24-54 and               */
+/* preflop_grid_generator.cu:47-77.                                          */
+/* ------------------------------------------------------------------------ */
+static int orc_straight_high(uint32_t m) {          /* f_str, :57-61 */
+    for (int r = 12; r >= 4; --r) {
+        uint32_t w = 0x1Fu << (r - 4);
+        if ((m & w) == w) return r;
+    }
+    if ((m & 0x100Fu) == 0x100Fu) return 3;
+    return -1;
+}
+
+uint32_t orc_score7(const uint8_t cards[7]) {
+    uint32_t sc[4] = {0, 0, 0, 0}, sm[4] = {0, 0, 0, 0}, rc[13], rm = 0;
+    memset(rc, 0, sizeof(rc));
+    for (int i = 0; i < 7; ++i) {                       /* :56 */
+        int c = cards[i], r = c / 4, s = c % 4;
+        sc[s]++; sm[s] |= 1u << r; rc[r]++; rm |= 1u << r;
+    }
+    for (int s = 0; s < 4; ++s) {                       /* :62-70 */
+        if (sc[s] >= 5) {
+            int sf = orc_straight_high(sm[s]);
+            if (sf != -1) return (8u << 24) | (uint32_t)sf;
+            uint32_t score = 5u << 24; int p = 0;
+            for (int r = 12; r >= 0 && p < 5; --r)
+                if (sm[s] & (1u << r)) { score |= (uint32_t)r << (4 * (4 - p)); ++p; }
+            return score;
+        }
+    }
+    int q = -1, t1 = -1, t2 = -1, p1 = -1, p2 = -1;     /* :71-75 */
+    for (int r = 12; r >= 0; --r) {
+        if (rc[r] == 4) q = r;
+        else if (rc[r] == 3) { if (t1 == -1) t1 = r; else if (t2 == -1) t2 = r; }
+        else if (rc[r] == 2) { if (p1 == -1) p1 = r; else if (p2 == -1) p2 = r; }
+    }
+    if (q != -1) return (7u << 24) | ((uint32_t)q << 4);                          /* :76 */
+    if (t1 != -1 && (t2 != -1 || p1 != -1))                                        /* :77 */
+        return (6u << 24) | ((uint32_t)t1 << 4) | (uint32_t)(t2 != -1 ? t2 : p1);
+    int st = orc_straight_high(rm);
+    if (st != -1) return (4u << 24) | (uint32_t)st;                                /* :78 */
+    if (t1 != -1) return (3u << 24) | ((uint32_t)t1 << 8);                         /* :79 */
+    if (p1 != -1 && p2 != -1) return (2u << 24) | ((uint32_t)p1 << 8) | ((uint32_t)p2 << 4); /* :80 */
+    if (p1 != -1) return (1u << 24) | ((uint32_t)p1 << 12);                        /* :81 */
+    return rm;                                                                     /* :82 */
+}
+
+void orc_eval7_batch(const uint8_t* cards7, uint32_t* out, int64_t n) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) out[i] = orc_score7(cards7 + 7 * i);
+}
+
+void orc_enumerate7(uint64_t hist[9], uint64_t* checksum) {
+    uint64_t h[9] = {0}, cs = 0;
+    /* colex order: largest card outermost; index = sum C(c_i, i+1). */
+    #pragma omp parallel
+    {
+        uint64_t lh[9] = {0}, lcs = 0;
+        #pragma omp for schedule(dynamic, 1)
+        for (int c6 = 6; c6 < 52; ++c6) {
+            /* index of the first subset whose largest card is c6 = C(c6, 7) */
+            uint64_t idx = 0;
+            { uint64_t b = 1; for (int k = 0; k < 7; ++k) b = b * (uint64_t)(c6 - k) / (uint64_t)(k + 1); idx = b; }
+            uint8_t c[7]; c[6] = (uint8_t)c6;
+            for (int c5 = 5; c5 < c6; ++c5) { c[5] = (uint8_t)c5;
+            for (int c4 = 4; c4 < c5; ++c4) { c[4] = (uint8_t)c4;
+            for (int c3 = 3; c3 < c4; ++c3) { c[3] = (uint8_t)c3;
+            for (int c2 = 2; c2 < c3; ++c2) { c[2] = (uint8_t)c2;
+            for (int c1 = 1; c1 < c2; ++c1) { c[1] = (uint8_t)c1;
+            for (int c0 = 0; c0 < c1; ++c0) { c[0] = (uint8_t)c0;
+                uint32_t s = orc_score7(c);
+                lh[s >> 24]++;
+                lcs += (uint64_t)s * (idx + 1);
+                ++idx;
+            }}}}}}
+        }
+        #pragma omp critical
+        { for (int k = 0; k < 9; ++k) h[k] += lh[k]; cs += lcs; }
+    }
+    for (int k = 0; k < 9; ++k) hist[k] = h[k];
+    *checksum = cs;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dumper: flop list (mtt_ev_dumper.cu:34-51), class map (:26-32),          */
+/* kernel_evaluate_flop_ev (:85-116), host aggregation (:141-168).          */
+/* ------------------------------------------------------------------------ */
+int orc_gen_flops(uint8_t* out) {
+    int n = 0;
+#define MC(r, s) ((uint8_t)((r) * 4 + (s)))
+#define PUSH(a, b, c, w) do { out[4*n] = (a); out[4*n+1] = (b); out[4*n+2] = (c); out[4*n+3] = (w); ++n; } while (0)
+    for (int r = 12; r >= 0; --r) PUSH(MC(r, 0), MC(r, 1), MC(r, 2), 4);
+    for (int rp = 12; rp >= 0; --rp) for (int rk = 12; rk >= 0; --rk) {
+        if (rp == rk) continue;
+        PUSH(MC(rp, 0), MC(rp, 1), MC(rk, 0), 12);
+        PUSH(MC(rp, 0), MC(rp, 1), MC(rk, 2), 12);
+    }
+    for (int r1 = 12; r1 >= 2; --r1) for (int r2 = r1 - 1; r2 >= 1; --r2) for (int r3 = r2 - 1; r3 >= 0; --r3) {
+        PUSH(MC(r1, 0), MC(r2, 0), MC(r3, 0), 4);
+        PUSH(MC(r1, 0), MC(r2, 0), MC(r3, 1), 12);
+        PUSH(MC(r1, 0), MC(r2, 1), MC(r3, 0), 12);
+        PUSH(MC(r1, 1), MC(r2, 0), MC(r3, 0), 12);
+        PUSH(MC(r1, 0), MC(r2, 1), MC(r3, 2), 24);
+    }
+#undef PUSH
+#undef MC
+    return n;
+}
+
+int orc_canonical_class(int c1, int c2) {
+    int r1 = c1 / 4, s1 = c1 % 4, r2 = c2 / 4, s2 = c2 % 4;
+    int hi = r1 > r2 ? r1 : r2, lo = r1 < r2 ? r1 : r2;
+    if (r1 == r2) return 12 - hi;
+    int b = (s1 == s2) ? 13 : 91;
+    for (int r = 12; r > hi; --r) b += r;
+    return b + (hi - 1 - lo);
+}
+
+void orc_flop_ev(const uint8_t flop[3], const float* reach0, const float* reach1,
+                 float* ev0, float* ev1) {
+    uint64_t fm = (1ull << flop[0]) | (1ull << flop[1]) | (1ull << flop[2]);
+    uint8_t deck[52]; int nd = 0;
+    for (int c = 0; c < 52; ++c) if (!((fm >> c) & 1)) deck[nd++] = (uint8_t)c;   /* :146 */
+    uint8_t ac1[1176], ac2[1176]; uint64_t am[1176]; int na = 0;
+    for (int c1 = 0; c1 < 52; ++c1) for (int c2 = c1 + 1; c2 < 52; ++c2) {        /* :149-152 */
+        uint64_t m = (1ull << c1) | (1ull << c2);
+        if (!(m & fm)) { ac1[na] = (uint8_t)c1; ac2[na] = (uint8_t)c2; am[na] = m; ++na; }
+    }
+    const float uni = 1.0f / 1176.0f;                                              /* :136 */
+    #pragma omp parallel for schedule(dynamic, 8)
+    for (int i = 0; i < 1176; ++i) {                                               /* :86-116 */
+        uint8_t h7[7] = {flop[0], flop[1], flop[2], ac1[i], ac2[i], 0, 0};
+        float t0 = 0.0f, t1 = 0.0f;
+        for (int j = 0; j < 1176; j += 4) {
+            if (am[i] & am[j]) continue;
+            uint8_t v7[7] = {flop[0], flop[1], flop[2], ac1[j], ac2[j], 0, 0};
+            uint64_t dead = am[i] | am[j];
+            int wins = 0, ties = 0, total = 0;
+            for (int r1 = 0; r1 < 47; r1 += 2) {
+                uint8_t turn = deck[r1];
+                if ((dead >> turn) & 1) continue;
+                h7[5] = turn; v7[5] = turn;
+                for (int r2 = r1 + 1; r2 < 47; r2 += 3) {
+                    uint8_t river = deck[r2];
+                    if ((dead >> river) & 1) continue;
+                    h7[6] = river; v7[6] = river;
+                    uint32_t sh = orc_score7(h7), sv = orc_score7(v7);
+                    if (sh > sv) wins += 2; else if (sh == sv) ties += 1;
+                    total += 2;
+                }
+            }
+            if (total > 0) {
+                float eq = (float)(wins + ties) / (float)total;
+                float r1j = reach1 ? reach1[j] : uni, r0j = reach0 ? reach0[j] : uni;
+                t0 = fmaf(r1j, fmaf(eq, 2.0f, -1.0f), t0);          /* :111, contracted */
+                t1 = fmaf(r0j, fmaf(1.0f - eq, 2.0f, -1.0f), t1);   /* :112, contracted */
+            }
+        }
+        ev0[i] = t0; ev1[i] = t1;
+    }
+}
+
+void orc_ev_dump(int f_begin, int f_end, float* out) {
+    uint8_t flops[1755 * 4];
+    orc_gen_flops(flops);
+    float* ev0 = (float*)malloc(1176 * sizeof(float));
+    float* ev1 = (float*)malloc(1176 * sizeof(float));
+    for (int f = f_begin; f < f_end; ++f) {
+        const uint8_t* fl = flops + 4 * f;
+        uint64_t fm = (1ull << fl[0]) | (1ull << fl[1]) | (1ull << fl[2]);
+        int cls[1176], na = 0;
+        for (int c1 = 0; c1 < 52; ++c1) for (int c2 = c1 + 1; c2 < 52; ++c2) {
+            uint64_t m = (1ull << c1) | (1ull << c2);
+            if (!(m & fm)) cls[na++] = orc_canonical_class(c1, c2);
+        }
+        orc_flop_ev(fl, NULL, NULL, ev0, ev1);
+        float* o = out + (size_t)(f - f_begin) * 4 * 2 * 169;
+        memset(o, 0, 4 * 2 * 169 * sizeof(float));
+        for (int scen = 0; scen < 4; ++scen) {                                     /* :160-168 */
+            float mult = 1.0f + 0.1f * (float)scen;
+            float* b = o + scen * 2 * 169;
+            for (int c = 0; c < 1176; ++c) {
+                b[cls[c]]       = b[cls[c]]       + ev0[c] * mult;
+                b[169 + cls[c]] = b[169 + cls[c]] + ev1[c] * mult;
+            }
+        }
+    }
+    free(ev0); free(ev1);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Showdown counts: kernel_gen_49_turn_matrices (honest:56-86) generalised   */
+/* to 3/4/5-card boards by exact enumeration of the missing board cards.     */
+/* ------------------------------------------------------------------------ */
+void orc_board_counts(const uint8_t* board, int nboard, const uint8_t* hands, int H,
+                      int32_t* w, int32_t* t, int32_t* l) {
+    uint64_t bm = 0;
+    for (int k = 0; k < nboard; ++k) bm |= 1ull << board[k];
+    uint8_t rest[52]; int nr = 0;
+    for (int c = 0; c < 52; ++c) if (!((bm >> c) & 1)) rest[nr++] = (uint8_t)c;
+    int need = 5 - nboard;
+    /* completions: list of (c_a, c_b) (c_b = 255 when need == 1; none when 0) */
+    int ncomp = need == 0 ? 1 : need == 1 ? nr : nr * (nr - 1) / 2;
+    uint8_t* ca = (uint8_t*)malloc((size_t)ncomp), *cb = (uint8_t*)malloc((size_t)ncomp);
+    {
+        int k = 0;
+        if (need == 0) { ca[0] = 255; cb[0] = 255; }
+        else if (need == 1) for (int a = 0; a < nr; ++a) { ca[k] = rest[a]; cb[k] = 255; ++k; }
+        else for (int a = 0; a < nr; ++a) for (int b = a + 1; b < nr; ++b) { ca[k] = rest[a]; cb[k] = rest[b]; ++k; }
+    }
+    uint32_t* sc = (uint32_t*)malloc((size_t)ncomp * (size_t)H * sizeof(uint32_t));
+    #pragma omp parallel for schedule(static)
+    for (int k = 0; k < ncomp; ++k) {
+        uint8_t c7[7];
+        for (int b = 0; b < nboard; ++b) c7[b] = board[b];
+        int nb = nboard;
+        if (ca[k] != 255) c7[nb++] = ca[k];
+        if (cb[k] != 255) c7[nb++] = cb[k];
+        for (int h = 0; h < H; ++h) {
+            c7[5] = hands[2 * h]; c7[6] = hands[2 * h + 1];
+            sc[(size_t)k * H + h] = orc_score7(c7);
+        }
+    }
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int i = 0; i < H; ++i) {
+        uint64_t mi = (1ull << hands[2 * i]) | (1ull << hands[2 * i + 1]);
+        for (int j = 0; j < H; ++j) {
+            uint64_t mj = (1ull << hands[2 * j]) | (1ull << hands[2 * j + 1]);
+            int32_t W = 0, T = 0, L = 0;
+            if (!(mi & mj) && !(mi & bm) && !(mj & bm)) {
+                uint64_t dead = mi | mj;
+                for (int k = 0; k < ncomp; ++k) {
+                    if (ca[k] != 255 && ((dead >> ca[k]) & 1)) continue;
+                    if (cb[k] != 255 && ((dead >> cb[k]) & 1)) continue;
+                    uint32_t si = sc[(size_t)k * H + i], sj = sc[(size_t)k * H + j];
+                    if (si > sj) ++W; else if (si == sj) ++T; else ++L;
+                }
+            }
+            w[(size_t)i * H + j] = W; t[(size_t)i * H + j] = T; l[(size_t)i * H + j] = L;
+        }
+    }
+    free(sc); free(ca); free(cb);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Heads-up CFR: kernel_forward_sweep (honest:88-126), kernel_evaluate_      */
+/* terminals (:128-196), kernel_backward_sweep (:198-249), with the DCFR     */
+/* discounting of kernel_dcfr_step (preflop_grid_generator.cu:387-410) in    */
+/* the standard discount-then-add form.                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct orc_ctx {
+    const orc_game* g;
+    int n;
+    int* parent;
+    int* dealt;          /* card dealt by the nearest chance ancestor, -1 if none */
+    uint64_t* hmask[2];  /* per hand card mask */
+    uint32_t* score[2];  /* [53][H_p]: score on board + dealt card (index 52 = no deal) */
+    int n_live;          /* cards not on the board */
+} orc_ctx;
+
+static int orc_ctx_init(orc_ctx* c, const orc_game* g) {
+    memset(c, 0, sizeof(*c));
+    c->g = g; c->n = g->n_nodes;
+    if (g->nboard != 5 && g->nboard != 4) return MTT_ERR_INVALID;
+    c->parent = (int*)malloc(sizeof(int) * (size_t)c->n);
+    c->dealt = (int*)malloc(sizeof(int) * (size_t)c->n);
+    for (int i = 0; i < c->n; ++i) { c->parent[i] = -1; c->dealt[i] = -1; }
+    for (int i = 0; i < c->n; ++i) {
+        const mtt_node* nd = &g->nodes[i];
+        if (nd->type == MTT_NODE_DECISION || nd->type == MTT_NODE_CHANCE)
+            for (int a = 0; a < nd->num_actions; ++a) c->parent[nd->children_offset + a] = i;
+    }
+    for (int i = 0; i < c->n; ++i) {   /* BFS order: parents first */
+        int p = c->parent[i];
+        if (p < 0) continue;
+        if (g->nodes[p].type == MTT_NODE_CHANCE) c->dealt[i] = g->nodes[i].turn_idx;
+        else c->dealt[i] = c->dealt[p];
+    }
+    uint64_t bm = 0;
+    for (int k = 0; k < g->nboard; ++k) bm |= 1ull << g->board[k];
+    c->n_live = 52 - g->nboard;
+    for (int p = 0; p < 2; ++p) {
+        int H = g->H[p];
+        c->hmask[p] = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(H > 0 ? H : 1));
+        c->score[p] = (uint32_t*)malloc(sizeof(uint32_t) * 53 * (size_t)(H > 0 ? H : 1));
+        for (int h = 0; h < H; ++h)
+            c->hmask[p][h] = (1ull << g->cards[p][2 * h]) | (1ull << g->cards[p][2 * h + 1]);
+        for (int d = 0; d < 53; ++d) {
+            int dc = d == 52 ? -1 : d;
+            if (g->nboard == 5 && dc != -1) continue;
+            if (g->nboard == 4 && (dc == -1 || ((bm >> dc) & 1))) continue;
+            for (int h = 0; h < H; ++h) {
+                uint8_t c7[7];
+                for (int k = 0; k < g->nboard; ++k) c7[k] = g->board[k];
+                if (g->nboard == 4) c7[4] = (uint8_t)dc;
+                c7[5] = g->cards[p][2 * h]; c7[6] = g->cards[p][2 * h + 1];
+                c->score[p][(size_t)d * H + h] = orc_score7(c7);
+            }
+        }
+    }
+    return MTT_OK;
+}
+
+static void orc_ctx_free(orc_ctx* c) {
+    free(c->parent); free(c->dealt);
+    for (int p = 0; p < 2; ++p) { free(c->hmask[p]); free(c->score[p]); }
+}
+
+/* Terminal values for player q against opponent reach ro (double math).    */
+/* sem: ORC_SEM_CORRECT or ORC_SEM_REFERENCE (honest:134-195 defects).      */
+static void orc_terminal_values(const orc_ctx* c, int node, int q, const double* ro,
+                                int sem, double* out) {
+    const orc_game* g = c->g;
+    const mtt_node* nd = &g->nodes[node];
+    int o = 1 - q, Hq = g->H[q], Ho = g->H[o];
+    int dealt = c->dealt[node];
+    uint64_t dm = dealt >= 0 ? (1ull << dealt) : 0;
+    if (nd->type == MTT_NODE_FOLD) {
+        int winner = (nd->active_mask == 1) ? 0 : 1;                       /* :135 */
+        double payoff = (q == winner) ? (double)nd->pot_size - (double)nd->committed[q]
+                                      : -(double)nd->committed[q];           /* :163-164 */
+        double tot = 0.0;
+        for (int j = 0; j < Ho; ++j) tot += ro[j];
+        for (int h = 0; h < Hq; ++h) {
+            double m;
+            if (sem == ORC_SEM_REFERENCE) m = tot;
+            else {
+                m = 0.0;
+                uint64_t mh = c->hmask[q][h] | dm;
+                for (int j = 0; j < Ho; ++j) if (!(c->hmask[o][j] & mh)) m += ro[j];
+            }
+            out[h] = payoff * m;
+        }
+        return;
+    }
+    /* showdown: honest:170-195 */
+    int d = (g->nboard == 5) ? 52 : dealt;
+    const uint32_t* sq = c->score[q] + (size_t)d * Hq;
+    const uint32_t* so = c->score[o] + (size_t)d * Ho;
+    double gain = (double)nd->pot_size - (double)nd->committed[q];
+    double loss = -(double)nd->committed[q];
+    double tie = 0.5 * (double)nd->pot_size - (double)nd->committed[q];
+    for (int h = 0; h < Hq; ++h) {
+        double acc = 0.0;
+        uint64_t mh = c->hmask[q][h];
+        if (sem == ORC_SEM_CORRECT) {
+            if (mh & dm) { out[h] = 0.0; continue; }
+            for (int j = 0; j < Ho; ++j) {
+                if (c->hmask[o][j] & (mh | dm)) continue;
+                double v = sq[h] > so[j] ? gain : (sq[h] == so[j] ? tie : loss);
+                acc += ro[j] * v;
+            }
+        } else {
+            for (int j = 0; j < Ho; ++j) {
+                int compat = !(c->hmask[o][j] & (mh | dm)) && !(mh & dm);
+                double eq = compat ? (sq[h] > so[j] ? 1.0 : (sq[h] == so[j] ? 0.5 : 0.0)) : 0.0;
+                if (q == 1) eq = 1.0 - eq;            /* :184-186 P1 uses 1 - eq(tid vs j) */
+                acc += ro[j] * (eq * gain + (1.0 - eq) * loss);
+            }
+        }
+        out[h] = acc;
+    }
+}
+
+int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
+                  float* R0, float* R1, float* S0, float* S1,
+                  float* root_cfv0, float* root_cfv1) {
+    orc_ctx c;
+    int st = orc_ctx_init(&c, g);
+    if (st) return st;
+    int n = g->n_nodes, H[2] = {g->H[0], g->H[1]};
+    float* R[2] = {R0, R1};
+    float* S[2] = {S0, S1};
+    for (int p = 0; p < 2; ++p) {
+        memset(R[p], 0, sizeof(float) * (size_t)g->rows[p] * (size_t)H[p]);
+        memset(S[p], 0, sizeof(float) * (size_t)g->rows[p] * (size_t)H[p]);
+    }
+    float* reach[2]; float* cfv[2]; float* sig[2];
+    for (int p = 0; p < 2; ++p) {
+        reach[p] = (float*)calloc((size_t)n * (size_t)H[p], sizeof(float));
+        cfv[p] = (float*)calloc((size_t)n * (size_t)H[p], sizeof(float));
+        sig[p] = (float*)calloc((size_t)g->rows[p] * (size_t)H[p] + 1, sizeof(float));
+    }
+    int Hmax = H[0] > H[1] ? H[0] : H[1];
+    double* ro = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
+    double* tv = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
+    float chance_div = (prm->semantics == ORC_SEM_REFERENCE) ? (float)(c.n_live - 2) : (float)(c.n_live - 4);
+
+    for (int t = 1; t <= prm->iters; ++t) {
+        float w_lin = (float)t;
+        double tm1 = (double)(t - 1);
+        float dpos = (float)(pow(tm1, (double)prm->alpha) / (pow(tm1, (double)prm->alpha) + 1.0));
+        float dneg = (float)(pow(tm1, (double)prm->beta) / (pow(tm1, (double)prm->beta) + 1.0));
+        float dstr = (float)pow(tm1 / (double)t, (double)prm->gamma);
+        /* forward (parents before children) */
+        for (int p = 0; p < 2; ++p) memcpy(reach[p], g->range[p], sizeof(float) * (size_t)H[p]);
+        for (int i = 0; i < n; ++i) {
+            const mtt_node* nd = &g->nodes[i];
+            if (nd->type == MTT_NODE_DECISION) {
+                int p = nd->player, o = 1 - p, A = nd->num_actions, row = nd->infoset_offset;
+                for (int h = 0; h < H[p]; ++h) {
+                    float pos[16], sum = 0.0f;
+                    for (int a = 0; a < A; ++a) {
+                        pos[a] = fmaxf(R[p][(size_t)(row + a) * H[p] + h], 0.0f);
+                        sum += pos[a];
+                    }
+                    float rp = reach[p][(size_t)i * H[p] + h];
+                    for (int a = 0; a < A; ++a) {
+                        float s = (sum > 1e-7f) ? pos[a] / sum : 1.0f / (float)A;   /* :117 */
+                        sig[p][(size_t)(row + a) * H[p] + h] = s;
+                        reach[p][(size_t)(nd->children_offset + a) * H[p] + h] = rp * s;
+                        float* sp = &S[p][(size_t)(row + a) * H[p] + h];
+                        if (prm->algo == ORC_ALGO_DCFR) *sp = fmaf(rp, s, *sp * dstr);
+                        else *sp = fmaf(w_lin * rp, s, *sp);                          /* :244 */
+                    }
+                }
+                for (int a = 0; a < A; ++a)
+                    memcpy(&reach[o][(size_t)(nd->children_offset + a) * H[o]],
+                           &reach[o][(size_t)i * H[o]], sizeof(float) * (size_t)H[o]);
+            } else if (nd->type == MTT_NODE_CHANCE) {                                /* :97-104 */
+                for (int a = 0; a < nd->num_actions; ++a) {
+                    int ch = nd->children_offset + a;
+                    uint64_t cm = 1ull << g->nodes[ch].turn_idx;
+                    for (int p = 0; p < 2; ++p)
+                        for (int h = 0; h < H[p]; ++h)
+                            reach[p][(size_t)ch * H[p] + h] =
+                                (c.hmask[p][h] & cm) ? 0.0f : reach[p][(size_t)i * H[p] + h];
+                }
+            }
+        }
+        /* terminals */
+        for (int i = 0; i < n; ++i) {
+            const mtt_node* nd = &g->nodes[i];
+            if (nd->type != MTT_NODE_FOLD && nd->type != MTT_NODE_SHOWDOWN) continue;
+            for (int q = 0; q < 2; ++q) {
+                int o = 1 - q;
+                for (int j = 0; j < H[o]; ++j) ro[j] = reach[o][(size_t)i * H[o] + j];
+                orc_terminal_values(&c, i, q, ro, prm->semantics, tv);
+                for (int h = 0; h < H[q]; ++h) cfv[q][(size_t)i * H[q] + h] = (float)tv[h];
+            }
+        }
+        /* backward (children before parents) */
+        for (int i = n - 1; i >= 0; --i) {
+            const mtt_node* nd = &g->nodes[i];
+            if (nd->type == MTT_NODE_DECISION) {                                     /* :220-246 */
+                int p = nd->player, o = 1 - p, A = nd->num_actions, row = nd->infoset_offset;
+                for (int h = 0; h < H[p]; ++h) {
+                    float v = 0.0f;
+                    for (int a = 0; a < A; ++a)
+                        v = fmaf(sig[p][(size_t)(row + a) * H[p] + h],
+                                 cfv[p][(size_t)(nd->children_offset + a) * H[p] + h], v);
+                    cfv[p][(size_t)i * H[p] + h] = v;
+                    for (int a = 0; a < A; ++a) {
+                        float qa = cfv[p][(size_t)(nd->children_offset + a) * H[p] + h];
+                        float* rr = &R[p][(size_t)(row + a) * H[p] + h];
+                        float inst = qa - v;
+                        if (prm->algo == ORC_ALGO_DCFR) {
+                            float disc = *rr * (*rr > 0.0f ? dpos : dneg);
+                            *rr = disc + inst;
+                        } else {
+                            *rr = fmaxf(0.0f, *rr + inst);                          /* :243 */
+                        }
+                    }
+                }
+                for (int h = 0; h < H[o]; ++h) {
+                    float so = 0.0f;
+                    for (int a = 0; a < A; ++a) so += cfv[o][(size_t)(nd->children_offset + a) * H[o] + h];
+                    cfv[o][(size_t)i * H[o] + h] = so;
+                }
+            } else if (nd->type == MTT_NODE_CHANCE) {                                /* :205-219 */
+                for (int p = 0; p < 2; ++p)
+                    for (int h = 0; h < H[p]; ++h) {
+                        float acc = 0.0f;
+                        for (int a = 0; a < nd->num_actions; ++a) {
+                            int ch = nd->children_offset + a;
+                            if (c.hmask[p][h] & (1ull << g->nodes[ch].turn_idx)) continue;
+                            acc += cfv[p][(size_t)ch * H[p] + h];
+                        }
+                        cfv[p][(size_t)i * H[p] + h] = acc / chance_div;
+                    }
+            }
+        }
+    }
+    if (root_cfv0) memcpy(root_cfv0, cfv[0], sizeof(float) * (size_t)H[0]);
+    if (root_cfv1) memcpy(root_cfv1, cfv[1], sizeof(float) * (size_t)H[1]);
+    for (int p = 0; p < 2; ++p) { free(reach[p]); free(cfv[p]); free(sig[p]); }
+    free(ro); free(tv);
+    orc_ctx_free(&c);
+    return MTT_OK;
+}
+
+/* Shared FP64 pass: values of both players when each plays `pol_p`
+ * (behaviour probabilities), plus best-response values. */
+static int orc_values_fp64(const orc_game* g, const double* pol0, const double* pol1,
+                           double* br_root0, double* br_root1,
+                           double* ev_root0, double* ev_root1, double* Z) {
+    orc_ctx c;
+    int st = orc_ctx_init(&c, g);
+    if (st) return st;
+    int n = g->n_nodes, H[2] = {g->H[0], g->H[1]};
+    const double* pol[2] = {pol0, pol1};
+    double *reach[2], *br[2], *ev[2];
+    for (int p = 0; p < 2; ++p) {
+        reach[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
+        br[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
+        ev[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
+        for (int h = 0; h < H[p]; ++h) reach[p][h] = g->range[p][h];
+    }
+    int Hmax = H[0] > H[1] ? H[0] : H[1];
+    double* tv = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
+    for (int i = 0; i < n; ++i) {
+        const mtt_node* nd = &g->nodes[i];
+        if (nd->type == MTT_NODE_DECISION) {
+            int p = nd->player, o = 1 - p;
+            for (int a = 0; a < nd->num_actions; ++a) {
+                int ch = nd->children_offset + a;
+                for (int h = 0; h < H[p]; ++h)
+                    reach[p][(size_t)ch * H[p] + h] = reach[p][(size_t)i * H[p] + h] *
+                        pol[p][(size_t)(nd->infoset_offset + a) * H[p] + h];
+                memcpy(&reach[o][(size_t)ch * H[o]], &reach[o][(size_t)i * H[o]], sizeof(double) * (size_t)H[o]);
+            }
+        } else if (nd->type == MTT_NODE_CHANCE) {
+            for (int a = 0; a < nd->num_actions; ++a) {
+                int ch = nd->children_offset + a;
+                uint64_t cm = 1ull << g->nodes[ch].turn_idx;
+                for (int p = 0; p < 2; ++p)
+                    for (int h = 0; h < H[p]; ++h)
+                        reach[p][(size_t)ch * H[p] + h] = (c.hmask[p][h] & cm) ? 0.0 : reach[p][(size_t)i * H[p] + h];
+            }
+        }
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        const mtt_node* nd = &g->nodes[i];
+        if (nd->type == MTT_NODE_FOLD || nd->type == MTT_NODE_SHOWDOWN) {
+            for (int q = 0; q < 2; ++q) {
+                int o = 1 - q;
+                orc_terminal_values(&c, i, q, &reach[o][(size_t)i * H[o]], ORC_SEM_CORRECT, tv);
+                for (int h = 0; h < H[q]; ++h) {
+                    br[q][(size_t)i * H[q] + h] = tv[h];
+                    ev[q][(size_t)i * H[q] + h] = tv[h];
+                }
+            }
+        } else if (nd->type == MTT_NODE_DECISION) {
+            int p = nd->player, o = 1 - p;
+            for (int h = 0; h < H[p]; ++h) {
+                double best = -1e300, v = 0.0;
+                for (int a = 0; a < nd->num_actions; ++a) {
+                    int ch = nd->children_offset + a;
+                    double b = br[p][(size_t)ch * H[p] + h];
+                    if (b > best) best = b;
+                    v += pol[p][(size_t)(nd->infoset_offset + a) * H[p] + h] * ev[p][(size_t)ch * H[p] + h];
+                }
+                br[p][(size_t)i * H[p] + h] = best;
+                ev[p][(size_t)i * H[p] + h] = v;
+            }
+            for (int h = 0; h < H[o]; ++h) {
+                double sb = 0.0, se = 0.0;
+                for (int a = 0; a < nd->num_actions; ++a) {
+                    int ch = nd->children_offset + a;
+                    sb += br[o][(size_t)ch * H[o] + h];
+                    se += ev[o][(size_t)ch * H[o] + h];
+                }
+                br[o][(size_t)i * H[o] + h] = sb;
+                ev[o][(size_t)i * H[o] + h] = se;
+            }
+        } else if (nd->type == MTT_NODE_CHANCE) {
+            double div = (double)(c.n_live - 4);
+            for (int p = 0; p < 2; ++p)
+                for (int h = 0; h < H[p]; ++h) {
+                    double sb = 0.0, se = 0.0;
+                    for (int a = 0; a < nd->num_actions; ++a) {
+                        int ch = nd->children_offset + a;
+                        if (c.hmask[p][h] & (1ull << g->nodes[ch].turn_idx)) continue;
+                        sb += br[p][(size_t)ch * H[p] + h];
+                        se += ev[p][(size_t)ch * H[p] + h];
+                    }
+                    br[p][(size_t)i * H[p] + h] = sb / div;
+                    ev[p][(size_t)i * H[p] + h] = se / div;
+                }
+        }
+    }
+    /* compatible range mass */
+    double z = 0.0;
+    for (int h = 0; h < H[0]; ++h) {
+        double m = 0.0;
+        for (int j = 0; j < H[1]; ++j) if (!(c.hmask[0][h] & c.hmask[1][j])) m += g->range[1][j];
+        z += (double)g->range[0][h] * m;
+    }
+    *Z = z;
+    if (br_root0) memcpy(br_root0, br[0], sizeof(double) * (size_t)H[0]);
+    if (br_root1) memcpy(br_root1, br[1], sizeof(double) * (size_t)H[1]);
+    if (ev_root0) memcpy(ev_root0, ev[0], sizeof(double) * (size_t)H[0]);
+    if (ev_root1) memcpy(ev_root1, ev[1], sizeof(double) * (size_t)H[1]);
+    for (int p = 0; p < 2; ++p) { free(reach[p]); free(br[p]); free(ev[p]); }
+    free(tv);
+    orc_ctx_free(&c);
+    return MTT_OK;
+}
+
+static double* orc_avg_policy(const orc_game* g, int p, const float* S) {
+    int H = g->H[p];
+    double* pol = (double*)calloc((size_t)g->rows[p] * (size_t)H + 1, sizeof(double));
+    for (int i = 0; i < g->n_nodes; ++i) {
+        const mtt_node* nd = &g->nodes[i];
+        if (nd->type != MTT_NODE_DECISION || nd->player != p) continue;
+        int A = nd->num_actions, row = nd->infoset_offset;
+        for (int h = 0; h < H; ++h) {
+            double sum = 0.0;
+            for (int a = 0; a < A; ++a) sum += (double)S[(size_t)(row + a) * H + h];
+            for (int a = 0; a < A; ++a)
+                pol[(size_t)(row + a) * H + h] = sum > 0.0 ? (double)S[(size_t)(row + a) * H + h] / sum : 1.0 / A;
+        }
+    }
+    return pol;
+}
+
+int orc_best_response(const orc_game* g, const float* S0, const float* S1, double out[6]) {
+    double* pol0 = orc_avg_policy(g, 0, S0);
+    double* pol1 = orc_avg_policy(g, 1, S1);
+    int H0 = g->H[0], H1 = g->H[1];
+    double* b0 = (double*)malloc(sizeof(double) * (size_t)(H0 + 1));
+    double* b1 = (double*)malloc(sizeof(double) * (size_t)(H1 + 1));
+    double* e0 = (double*)malloc(sizeof(double) * (size_t)(H0 + 1));
+    double* e1 = (double*)malloc(sizeof(double) * (size_t)(H1 + 1));
+    double Z = 0.0;
+    int st = orc_values_fp64(g, pol0, pol1, b0, b1, e0, e1, &Z);
+    if (st == MTT_OK) {
+        double br0 = 0, br1 = 0, ev0 = 0, ev1 = 0;
+        for (int h = 0; h < H0; ++h) { br0 += g->range[0][h] * b0[h]; ev0 += g->range[0][h] * e0[h]; }
+        for (int h = 0; h < H1; ++h) { br1 += g->range[1][h] * b1[h]; ev1 += g->range[1][h] * e1[h]; }
+        double zz = Z > 0 ? Z : 1.0;
+        out[0] = br0 / zz; out[1] = br1 / zz; out[2] = ev0 / zz; out[3] = ev1 / zz; out[4] = Z;
+        out[5] = 0.5 * (out[0] + out[1]) / (double)g->nodes[0].pot_size;
+    }
+    free(pol0); free(pol1); free(b0); free(b1); free(e0); free(e1);
+    return st;
+}
+
+int orc_strategy_values(const orc_game* g, const float* sigma0, const float* sigma1,
+                        double* out_cfv0, double* out_cfv1, double* ev_out) {
+    int rows0 = g->rows[0], rows1 = g->rows[1];
+    double* pol0 = (double*)malloc(sizeof(double) * ((size_t)rows0 * (size_t)g->H[0] + 1));
+    double* pol1 = (double*)malloc(sizeof(double) * ((size_t)rows1 * (size_t)g->H[1] + 1));
+    for (size_t k = 0; k < (size_t)rows0 * (size_t)g->H[0]; ++k) pol0[k] = sigma0[k];
+    for (size_t k = 0; k < (size_t)rows1 * (size_t)g->H[1]; ++k) pol1[k] = sigma1[k];
+    double Z = 0.0;
+    int st = orc_values_fp64(g, pol0, pol1, NULL, NULL, out_cfv0, out_cfv1, &Z);
+    if (st == MTT_OK && ev_out) {
+        double ev = 0.0;
+        for (int h = 0; h < g->H[0]; ++h) ev += (double)g->range[0][h] * out_cfv0[h];
+        *ev_out = ev;
+    }
+    free(pol0); free(pol1);
+    return st;
+}

@@ -1,0 +1,163 @@
+"""ctypes binding of the CPU oracle (oracle/libmtt_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py, as the checker and the timed CPU baseline.  The product
+(libmtt_b200.so and the mtt-gpu-solver_b200 package) never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmtt_oracle.so")
+_lib = None
+
+
+def build():
+    r = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB_PATH
+
+
+class Game(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int32), ("rows", ctypes.c_int32 * 2),
+                ("board", ctypes.c_void_p), ("nboard", ctypes.c_int32), ("H", ctypes.c_int32 * 2),
+                ("cards", ctypes.c_void_p * 2), ("range", ctypes.c_void_p * 2)]
+
+
+class CfrParams(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("algo", ctypes.c_int32), ("alpha", ctypes.c_float),
+                ("beta", ctypes.c_float), ("gamma", ctypes.c_float), ("semantics", ctypes.c_int32)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.orc_score7.argtypes = [vp]; L.orc_score7.restype = ctypes.c_uint32
+        L.orc_eval7_batch.argtypes = [vp, vp, ctypes.c_int64]
+        L.orc_enumerate7.argtypes = [vp, vp]
+        L.orc_gen_flops.argtypes = [vp]; L.orc_gen_flops.restype = ctypes.c_int
+        L.orc_canonical_class.argtypes = [ctypes.c_int, ctypes.c_int]; L.orc_canonical_class.restype = ctypes.c_int
+        L.orc_flop_ev.argtypes = [vp, vp, vp, vp, vp]
+        L.orc_ev_dump.argtypes = [ctypes.c_int, ctypes.c_int, vp]
+        L.orc_board_counts.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp, vp]
+        L.orc_cfr_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]; L.orc_cfr_solve.restype = ctypes.c_int
+        L.orc_best_response.argtypes = [vp, vp, vp, vp]; L.orc_best_response.restype = ctypes.c_int
+        L.orc_strategy_values.argtypes = [vp, vp, vp, vp, vp, vp]; L.orc_strategy_values.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def eval7(cards7):
+    c = np.ascontiguousarray(cards7, dtype=np.uint8)
+    out = np.zeros(len(c), dtype=np.uint32)
+    lib().orc_eval7_batch(c.ctypes.data, out.ctypes.data, len(c))
+    return out
+
+
+def enumerate7():
+    hist = np.zeros(9, dtype=np.uint64)
+    cs = ctypes.c_uint64()
+    lib().orc_enumerate7(hist.ctypes.data, ctypes.byref(cs))
+    return hist, cs.value
+
+
+def gen_flops():
+    out = np.zeros(1755 * 4, dtype=np.uint8)
+    n = lib().orc_gen_flops(out.ctypes.data)
+    return out.reshape(-1, 4)[:n]
+
+
+def flop_ev(flop3, reach0=None, reach1=None):
+    f = np.ascontiguousarray(flop3, dtype=np.uint8)
+    e0 = np.zeros(1176, np.float32); e1 = np.zeros(1176, np.float32)
+    r0 = np.ascontiguousarray(reach0, np.float32) if reach0 is not None else None
+    r1 = np.ascontiguousarray(reach1, np.float32) if reach1 is not None else None
+    lib().orc_flop_ev(f.ctypes.data, r0.ctypes.data if r0 is not None else None,
+                      r1.ctypes.data if r1 is not None else None, e0.ctypes.data, e1.ctypes.data)
+    return e0, e1
+
+
+def ev_dump(f_begin, f_end):
+    out = np.zeros((f_end - f_begin, 4, 2, 169), np.float32)
+    lib().orc_ev_dump(f_begin, f_end, out.ctypes.data)
+    return out
+
+
+def board_counts(board, hands):
+    b = np.ascontiguousarray(board, np.uint8)
+    h = np.ascontiguousarray(hands, np.uint8)
+    H = len(h)
+    W = np.zeros((H, H), np.int32); T = np.zeros((H, H), np.int32); L = np.zeros((H, H), np.int32)
+    lib().orc_board_counts(b.ctypes.data, len(b), h.ctypes.data, H, W.ctypes.data, T.ctypes.data, L.ctypes.data)
+    return W, T, L
+
+
+class _GameHolder:
+    def __init__(self, sub):
+        from numpy.lib import recfunctions  # noqa: F401  (numpy only)
+        self.nodes = np.ascontiguousarray(sub["nodes"])
+        self.board = np.ascontiguousarray(np.asarray(sub["board"], np.uint8))
+        self.cards = [np.ascontiguousarray(_combo_cards(sub[f"combos{p}"])) for p in (0, 1)]
+        self.range = [np.ascontiguousarray(sub[f"range{p}"], np.float32) for p in (0, 1)]
+        g = Game()
+        g.nodes = self.nodes.ctypes.data
+        g.n_nodes = len(self.nodes)
+        g.rows[0], g.rows[1] = int(sub["rows"][0]), int(sub["rows"][1])
+        g.board = self.board.ctypes.data
+        g.nboard = len(self.board)
+        g.H[0], g.H[1] = len(self.range[0]), len(self.range[1])
+        g.cards[0], g.cards[1] = self.cards[0].ctypes.data, self.cards[1].ctypes.data
+        g.range[0], g.range[1] = self.range[0].ctypes.data, self.range[1].ctypes.data
+        self.g = g
+        self.rows = (g.rows[0], g.rows[1])
+        self.H = (g.H[0], g.H[1])
+
+
+_CC = np.array([(a, b) for a in range(52) for b in range(a + 1, 52)], dtype=np.uint8)
+
+
+def _combo_cards(ids):
+    return _CC[np.asarray(ids, dtype=np.int64)]
+
+
+def cfr_solve(sub, iters, algo=0, alpha=1.5, beta=0.0, gamma=2.0, semantics=0):
+    gh = _GameHolder(sub)
+    p = CfrParams(int(iters), int(algo), float(alpha), float(beta), float(gamma), int(semantics))
+    R0 = np.zeros((gh.rows[0], gh.H[0]), np.float32); R1 = np.zeros((gh.rows[1], gh.H[1]), np.float32)
+    S0 = np.zeros_like(R0); S1 = np.zeros_like(R1)
+    c0 = np.zeros(gh.H[0], np.float32); c1 = np.zeros(gh.H[1], np.float32)
+    st = lib().orc_cfr_solve(ctypes.byref(gh.g), ctypes.byref(p), R0.ctypes.data, R1.ctypes.data, S0.ctypes.data,
+                             S1.ctypes.data, c0.ctypes.data, c1.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_cfr_solve status {st}")
+    return {"R0": R0, "R1": R1, "S0": S0, "S1": S1, "cfv0": c0, "cfv1": c1}
+
+
+def best_response(sub, S0, S1):
+    gh = _GameHolder(sub)
+    out = np.zeros(6, np.float64)
+    s0 = np.ascontiguousarray(S0, np.float32); s1 = np.ascontiguousarray(S1, np.float32)
+    st = lib().orc_best_response(ctypes.byref(gh.g), s0.ctypes.data, s1.ctypes.data, out.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_best_response status {st}")
+    return out
+
+
+def strategy_values(sub, sigma0, sigma1):
+    gh = _GameHolder(sub)
+    s0 = np.ascontiguousarray(sigma0, np.float32); s1 = np.ascontiguousarray(sigma1, np.float32)
+    c0 = np.zeros(gh.H[0], np.float64); c1 = np.zeros(gh.H[1], np.float64)
+    ev = ctypes.c_double()
+    st = lib().orc_strategy_values(ctypes.byref(gh.g), s0.ctypes.data, s1.ctypes.data, c0.ctypes.data,
+                                   c1.ctypes.data, ctypes.byref(ev))
+    if st:
+        raise RuntimeError(f"orc_strategy_values status {st}")
+    return c0, c1, ev.value

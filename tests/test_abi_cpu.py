@@ -1,0 +1,112 @@
+"""C ABI and host logic that run without a GPU: exports, trees, validation."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+
+def test_library_exports_every_declared_symbol(mtt):
+    import subprocess
+    L = mtt.lib()
+    declared = mtt._lib.exported_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", mtt._lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (mtt_\w+)", out))
+    assert set(declared) <= exported
+    assert mtt.lib().mtt_version().startswith(b"mtt-b200")
+    assert mtt.lib().mtt_status_string(0) == b"ok"
+
+
+def _check_tree(mtt, nodes, rows):
+    assert mtt.validate_tree(nodes, rows) == 0
+    n = len(nodes)
+    seen = np.zeros(n, bool)
+    for i, nd in enumerate(nodes):
+        if nd["type"] in (mtt.NODE_DECISION, mtt.NODE_CHANCE):
+            f, a = nd["children_offset"], nd["num_actions"]
+            assert f > i and f + a <= n
+            assert not seen[f:f + a].any()
+            seen[f:f + a] = True
+            for c in range(f, f + a):
+                assert nodes[c]["depth"] == nd["depth"] + 1
+        if nd["type"] == mtt.NODE_SHOWDOWN:
+            assert abs(nd["committed"][0] - nd["committed"][1]) < 1e-3
+        if nd["type"] != mtt.NODE_CHANCE:
+            assert abs(nd["pot_size"] - nd["committed"].sum()) < 1e-3
+    assert seen[1:].all()
+
+
+def test_river_tree_config0_shape(mtt):
+    nodes, rows, depth = mtt.build_tree(100, 200, [0.5, 1.0], raise_cap=1)
+    _check_tree(mtt, nodes, rows)
+    assert nodes[0]["num_actions"] == 4            # check, 50, 100, all-in
+    assert nodes[0]["player"] == 0
+    assert rows[0] == rows[1]
+    # fold payoffs are zero-sum: winner gains the loser's commitment
+    for nd in nodes[nodes["type"] == mtt.NODE_FOLD]:
+        w = 0 if nd["active_mask"] == 1 else 1
+        assert nd["pot_size"] - nd["committed"][w] == pytest.approx(nd["committed"][1 - w])
+    # all-in never exceeds the stack
+    assert (nodes["committed"] <= 50 + 200 + 1e-3).all()
+
+
+@pytest.mark.parametrize("sizes,cap,pot,stack", [([0.853], 1, 37.8, 31.8), ([0.25, 0.5, 1.0, 2.0], 3, 20, 240),
+                                                 ([1.992], 3, 144.5, 1195.0), ([0.347, 0.579, 1.525], 2, 138.3, 964)])
+def test_river_tree_random_specs(mtt, sizes, cap, pot, stack):
+    nodes, rows, depth = mtt.build_tree(pot, stack, sizes, raise_cap=cap)
+    _check_tree(mtt, nodes, rows)
+    assert nodes["num_actions"].max() <= 8
+
+
+def test_turn_tree_has_river_chance_layer(mtt):
+    board = [0, 13, 26, 39]
+    nodes, rows, depth = mtt.build_tree(60, 470, [0.33, 0.75, 1.5], raise_cap=2, street=4, board=board)
+    _check_tree(mtt, nodes, rows)
+    ch = nodes[nodes["type"] == mtt.NODE_CHANCE]
+    assert len(ch) > 0 and (ch["num_actions"] == 48).all()
+    for nd in ch:
+        kids = nodes[nd["children_offset"]:nd["children_offset"] + 48]
+        assert sorted(kids["turn_idx"].tolist()) == [c for c in range(52) if c not in board]
+
+
+def test_validation_rejects_malformed_trees(mtt):
+    nodes, rows, _ = mtt.build_tree(100, 200, [0.5, 1.0], raise_cap=1)
+    bad = nodes.copy(); bad[0]["children_offset"] = 0
+    assert mtt.validate_tree(bad, rows) != 0                   # child before parent / cycle
+    bad = nodes.copy(); bad[0]["children_offset"] = len(nodes) - 1
+    assert mtt.validate_tree(bad, rows) != 0                   # children out of range
+    bad = nodes.copy(); bad[0]["infoset_offset"] = rows[0]
+    assert mtt.validate_tree(bad, rows) != 0                   # regret rows out of range
+    bad = nodes.copy(); bad[nodes["type"] == mtt.NODE_FOLD][0]["active_mask"] = 3
+    i = int(np.nonzero(nodes["type"] == mtt.NODE_FOLD)[0][0]); bad = nodes.copy(); bad[i]["active_mask"] = 3
+    assert mtt.validate_tree(bad, rows) != 0
+    assert mtt.validate_tree(nodes, rows) == 0
+
+
+def test_invalid_arguments_return_status_not_crash(mtt):
+    L = mtt.lib()
+    assert L.mtt_eval7(None, None, -1, None) == 1
+    assert L.mtt_board_showdown_counts(None, 7, None, 10, None, None, None, None) == 1
+    assert L.mtt_batch_create(None, 0, None) == 1
+    assert L.mtt_batch_solve(None, None, None) == 1
+    sp = mtt.make_spec(-1, 100, [0.5])
+    n = ctypes.c_int32(); rows = (ctypes.c_int32 * 2)(); d = ctypes.c_int32()
+    assert L.mtt_tree_build(ctypes.byref(sp), None, 0, ctypes.byref(n), rows, ctypes.byref(d)) == 1
+
+
+def test_canonical_flops_host(mtt, orc):
+    assert (mtt.canonical_flops() == orc.gen_flops()).all()
+
+
+def test_workload_config2_shapes(wl):
+    subs = wl.river_batch(n=64, seed=2)
+    assert len(subs) == 64
+    for g in subs:
+        for p in (0, 1):
+            c = g[f"combos{p}"]
+            assert 200 <= len(c) <= 1081 and (np.diff(c.astype(int)) > 0).all()
+            assert (g[f"range{p}"] > 0).all()
+        assert g["nodes"]["num_actions"].max() <= 8
