@@ -171,8 +171,20 @@ typedef struct mtt_solve_params {
     int32_t algo;
     float   alpha, beta, gamma;   /* DCFR only */
     int32_t semantics;
-    int32_t threads;              /* CTA size of the batched kernel (64/128/256); 0 = autotuned */
+    int32_t threads;              /* CTA size of the sweep kernels (64/128/256); 0 = autotuned.
+                                     Results do not depend on it. */
     int32_t exploitability;       /* 1: FP64 best-response pass after the iterations */
+    int32_t alternate;            /* 1: alternating updates (CFR+ as published: P0's pass, then
+                                     P1's against P0's new strategy); 0: simultaneous updates of
+                                     both players per sweep, as the reference kernels do */
+    float   avg_power;            /* CFR+ strategy-sum weight t^avg_power (1: linear averaging,
+                                     2: quadratic); DCFR uses gamma instead */
+    float   target_expl;          /* > 0 (with exploitability = 1 and max_iters > iters): after
+                                     `iters` iterations, subgames whose exploitability is above
+                                     target_expl (fraction of the starting pot) keep iterating in
+                                     chunks of chunk_iters until they pass or reach max_iters */
+    int32_t max_iters;
+    int32_t chunk_iters;          /* 0: iters / 2 */
 } mtt_solve_params;
 
 /* One heads-up subgame.  combos[p] ascending combo ids (0..1325) of player
@@ -194,22 +206,31 @@ typedef struct mtt_batch mtt_batch;
  * Synchronous.  Per subgame the layout is reach/CFV vectors per node, R and S
  * per regret row, and per-board showdown rank tables. */
 int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** out);
-/* Solve every subgame from zero regrets: one persistent kernel, one CTA per
- * subgame at a time from a work queue (largest first), then (optionally) the
- * FP64 best-response kernel.  Asynchronous on stream. */
+/* Solve every subgame from zero regrets.  Each iteration is a sequence of
+ * level-synchronous launches over the whole batch (forward levels,
+ * terminals, backward levels per pass); then, optionally, the FP64
+ * best-response pass.  Asynchronous on stream. */
 int mtt_batch_solve(mtt_batch* b, const mtt_solve_params* prm, void* stream);
-/* Same work as mtt_batch_solve, replayed from a CUDA graph captured on the
- * first call for these params. */
+/* Same work as mtt_batch_solve, with one iteration captured as a CUDA graph
+ * (on the first call for these params) and replayed per iteration. */
 int mtt_batch_solve_graph(mtt_batch* b, const mtt_solve_params* prm, void* stream);
 /* Per subgame: [0] BR value of P0, [1] BR of P1, [2] EV of P0 under the
  * average strategies, [3] EV of P1 (per unit of compatible range mass),
  * [4] compatible range mass Z, [5] exploitability (BR0+BR1)/2 / starting pot.
  * Waits for the stream. */
 int mtt_batch_results(mtt_batch* b, double* h_out, void* stream);
+/* Iterations run per subgame by the last solve (iters, plus continuation
+ * chunks when a target exploitability was set).  h_out: n entries. */
+int mtt_batch_iterations(mtt_batch* b, int32_t* h_out);
 /* Regrets R_p, strategy sums S_p ([rows_p][H_p]) and last-iteration root
  * CFVs (cfv_p[H_p]) of subgame s; any pointer may be NULL.  Synchronous. */
 int mtt_batch_read(mtt_batch* b, int32_t s, float* h_R0, float* h_R1, float* h_S0, float* h_S1,
                    float* h_cfv0, float* h_cfv1);
+/* Per-node vectors of subgame s after the last iteration: h_reach[n][p][H_p]
+ * (player p's reach at node n, from the slot that holds it) and
+ * h_cfv[n][p][H_p] (counterfactual values), both [n_nodes][H0 + H1] with
+ * player 0's hands first.  Either pointer may be NULL.  Synchronous. */
+int mtt_batch_read_vectors(mtt_batch* b, int32_t s, float* h_reach, float* h_cfv);
 /* Device bytes held, and algorithmic bytes of one CFR iteration over the whole
  * batch (R,S read+write per action-hand; reach and CFV written and read once
  * per player-hand per node). */

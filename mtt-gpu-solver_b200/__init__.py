@@ -169,10 +169,14 @@ def ev_dump(flops3, stream=None):
 
 # ------------------------------------------------------------------ solving
 def solve_params(iters=1000, algo=ALGO_CFRPLUS, alpha=1.5, beta=0.0, gamma=2.0, semantics=SEM_CORRECT,
-                 threads=0, exploitability=True):
+                 threads=0, exploitability=True, alternate=True, avg_power=1.0, target_expl=0.0, max_iters=0,
+                 chunk_iters=0):
     p = SolveParams()
     p.iters, p.algo, p.alpha, p.beta, p.gamma = int(iters), int(algo), float(alpha), float(beta), float(gamma)
     p.semantics, p.threads, p.exploitability = int(semantics), int(threads), 1 if exploitability else 0
+    p.alternate = 1 if alternate else 0
+    p.avg_power = float(avg_power)
+    p.target_expl, p.max_iters, p.chunk_iters = float(target_expl), int(max_iters), int(chunk_iters)
     return p
 
 
@@ -222,6 +226,11 @@ class RiverBatch:
         check("mtt_batch_results", lib().mtt_batch_results(self._h, out.ctypes.data, _stream(stream)))
         return out
 
+    def iterations(self):
+        out = np.zeros(self.n, dtype=np.int32)
+        check("mtt_batch_iterations", lib().mtt_batch_iterations(self._h, out.ctypes.data))
+        return out
+
     def read(self, s):
         rows0, rows1, H0, H1 = self.meta[s]
         R0 = np.zeros((rows0, H0), np.float32); R1 = np.zeros((rows1, H1), np.float32)
@@ -230,6 +239,15 @@ class RiverBatch:
         check("mtt_batch_read", lib().mtt_batch_read(self._h, s, R0.ctypes.data, R1.ctypes.data, S0.ctypes.data,
                                                      S1.ctypes.data, c0.ctypes.data, c1.ctypes.data))
         return {"R0": R0, "R1": R1, "S0": S0, "S1": S1, "cfv0": c0, "cfv1": c1}
+
+    def read_vectors(self, s, n_nodes):
+        """Per-node reach and counterfactual values of subgame s: two
+        [n_nodes, H0 + H1] arrays (player 0's hands first)."""
+        rows0, rows1, H0, H1 = self.meta[s]
+        reach = np.zeros((n_nodes, H0 + H1), np.float32)
+        cfv = np.zeros((n_nodes, H0 + H1), np.float32)
+        check("mtt_batch_read_vectors", lib().mtt_batch_read_vectors(self._h, s, reach.ctypes.data, cfv.ctypes.data))
+        return reach, cfv
 
     def info(self):
         db = ctypes.c_int64()

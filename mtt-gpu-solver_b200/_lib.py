@@ -38,7 +38,9 @@ class TreeSpec(ctypes.Structure):
 class SolveParams(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("algo", ctypes.c_int32), ("alpha", ctypes.c_float),
                 ("beta", ctypes.c_float), ("gamma", ctypes.c_float), ("semantics", ctypes.c_int32),
-                ("threads", ctypes.c_int32), ("exploitability", ctypes.c_int32)]
+                ("threads", ctypes.c_int32), ("exploitability", ctypes.c_int32), ("alternate", ctypes.c_int32),
+                ("avg_power", ctypes.c_float), ("target_expl", ctypes.c_float), ("max_iters", ctypes.c_int32),
+                ("chunk_iters", ctypes.c_int32)]
 
 
 class Subgame(ctypes.Structure):
@@ -82,6 +84,8 @@ def lib():
         "mtt_batch_solve_graph": ([vp, vp, vp], ctypes.c_int),
         "mtt_batch_results": ([vp, vp, vp], ctypes.c_int),
         "mtt_batch_read": ([vp, i32, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_iterations": ([vp, vp], ctypes.c_int),
+        "mtt_batch_read_vectors": ([vp, i32, vp, vp], ctypes.c_int),
         "mtt_batch_info": ([vp, vp, vp], ctypes.c_int),
         "mtt_batch_autotune": ([vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_destroy": ([vp], ctypes.c_int),

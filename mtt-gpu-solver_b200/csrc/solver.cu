@@ -1,21 +1,27 @@
 // solver.cu — batched heads-up CFR+/DCFR solver and its FP64 best response.
 //
-// One persistent kernel solves every subgame of a batch: each CTA pulls the
-// next subgame (largest first) from an atomic work queue and runs all
-// iterations on it.  Inside a CTA each thread owns fixed groups of 4 hands
-// (float4), so the forward sweep (regret matching, reach, strategy sums) and
-// the backward sweep (counterfactual values, regret update) walk the tree
-// node by node with NO barriers: a thread only ever reads values it wrote.
-// Only terminals mix hands; they are evaluated CTA-wide with one exclusive
-// prefix scan per terminal over the opponent reach in rank order and in
-// per-card rank order, from which wins, ties and losses with card removal
-// are O(1) differences (no 1326x1326 matrices).
+// Level-synchronous over the whole batch: every tree level of every subgame
+// is one flat list of warp tasks (subgame, node, 32 groups of 4 hands), so a
+// launch streams all subgames' nodes of that depth through HBM with float4
+// accesses and no intra-kernel barriers.  An iteration is
+//   [forward levels 0..D] [terminals] [backward levels D..0]   per pass,
+// one pass per player with alternating updates (CFR+ as published) or one
+// pass updating both (the reference kernels' simultaneous updates), captured
+// once as a CUDA graph and replayed for every iteration; a device counter
+// carries the iteration number into the kernels.
+//
+// Terminals are one warp each.  Fold values need the opponent's total and
+// per-card reach mass; showdown values need one exclusive prefix scan of the
+// opponent reach in rank order and in per-card rank order, from which wins,
+// ties and losses with card removal are O(1) differences.  The scan is split
+// over lanes by the opponent's hand count only, so results never depend on
+// the launch configuration.
 //
 // Update rules follow the reference kernels: kernel_forward_sweep
-// (honest_multistreet_solver.cu:88-126), kernel_backward_sweep (:198-249),
-// kernel_4way_* (multiway_4way_engine.cu:41-83,219-257) and the DCFR weights
-// of kernel_dcfr_step (preflop_grid_generator.cu:387-410, in the
-// discount-then-add form).
+// (honest_multistreet_solver.cu:88-126), kernel_evaluate_terminals
+// (:128-196), kernel_backward_sweep (:198-249), kernel_4way_* (multiway_4way_
+// engine.cu:41-83,219-257) and the DCFR weights of kernel_dcfr_step
+// (preflop_grid_generator.cu:387-410, in the discount-then-add form).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -23,6 +29,7 @@
 #include <thread>
 #include <vector>
 
+#include "mtt_bulk.cuh"
 #include "mtt_common.h"
 #include "mtt_device.cuh"
 #include "solver_impl.cuh"
@@ -40,27 +47,38 @@ __host__ __device__ __forceinline__ int tab_variant(int river, int dealt) {
 
 // ====================================================================== device
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
-__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+    return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
 __device__ __forceinline__ float4 mul4(float4 a, float4 b) {
     return make_float4(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z), __fmul_rn(a.w, b.w));
 }
-__device__ __forceinline__ float4 max04(float4 a) { return make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f)); }
+__device__ __forceinline__ float4 max04(float4 a) {
+    return make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
+}
 __device__ __forceinline__ float rm1(float pos, float sum, float invA) { return sum > 1e-7f ? __fdiv_rn(pos, sum) : invA; }
 __device__ __forceinline__ float4 rm4(float4 pos, float4 sum, float invA) {
-    return make_float4(rm1(pos.x, sum.x, invA), rm1(pos.y, sum.y, invA), rm1(pos.z, sum.z, invA), rm1(pos.w, sum.w, invA));
+    return make_float4(rm1(pos.x, sum.x, invA), rm1(pos.y, sum.y, invA), rm1(pos.z, sum.z, invA),
+                       rm1(pos.w, sum.w, invA));
 }
 __device__ __forceinline__ float4 fma4(float4 a, float4 b, float4 c) {
-    return make_float4(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y), __fmaf_rn(a.z, b.z, c.z), __fmaf_rn(a.w, b.w, c.w));
+    return make_float4(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y), __fmaf_rn(a.z, b.z, c.z),
+                       __fmaf_rn(a.w, b.w, c.w));
 }
 __device__ __forceinline__ float cfrplus1(float r, float inst) { return fmaxf(0.0f, __fadd_rn(r, inst)); }
 __device__ __forceinline__ float dcfr1(float r, float inst, float dpos, float dneg) {
     return __fadd_rn(__fmul_rn(r, r > 0.0f ? dpos : dneg), inst);
 }
 
-struct BatchDev {
+struct Task {        // one warp: groups [g0, g0 + 32) of float4 hand groups at one node
+    int node;        // global node index
+    int sub;         // subgame
+    int g0;
+    int pad;
+};
+
+struct SolveDev {
     const SubDesc* desc;
-    int n_sub;
-    const int* order;
     const DNode* nodes;
     const uint8_t* tabs;
     const uint16_t* hcards;
@@ -71,78 +89,15 @@ struct BatchDev {
     double* darena;
     double* results;
     const float* iter_tab;
-    int iters, algo, semantics;
-    int* queue;
+    int* iter;          // device iteration counter, 1-based
+    int* err;           // bit 0: a bounded wait for a bulk copy gave up
+    int algo, semantics;
 };
 
-// per-player selects (runtime-indexed local arrays would live in local memory)
 #define HP(p) ((p) ? sd.Hp1 : sd.Hp0)
+#define HH(p) ((p) ? sd.H1 : sd.H0)
 #define OFF(p) ((p) ? sd.Hp0 : 0)
-#define RP(p) (a.R + ((p) ? sd.rs_base1 : sd.rs_base0))
-#define SP(p) (a.S + ((p) ? sd.rs_base1 : sd.rs_base0))
-
-// exclusive scan of x[0..n) in place, x[n] = total; all threads of the CTA
-template <typename T>
-__device__ void block_scan_excl(T* x, int n, T* wbuf, int tid, int B) {
-    const int C = (n + B - 1) / B;
-    const int s = min(tid * C, n), e = min(s + C, n);
-    T loc = T(0);
-    for (int k = s; k < e; ++k) loc += x[k];
-    const int lane = tid & 31, wid = tid >> 5, nw = B >> 5;
-    T inc = loc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-        if (lane >= o) inc += t;
-    }
-    T exc = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-    if (lane == 0) exc = T(0);
-    if (lane == 31) wbuf[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-        T w = lane < nw ? wbuf[lane] : T(0);
-        T wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T t = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        T we = __shfl_up_sync(0xFFFFFFFFu, wi, 1);
-        if (lane == 0) we = T(0);
-        if (lane < nw) wbuf[lane] = we;
-        if (lane == nw - 1) wbuf[32] = wi;
-    }
-    __syncthreads();
-    T run = wbuf[wid] + exc;
-    for (int k = s; k < e; ++k) {
-        const T v = x[k];
-        x[k] = run;
-        run += v;
-    }
-    if (tid == 0) x[n] = wbuf[32];
-    __syncthreads();
-}
-
-template <typename T>
-__device__ T block_sum(T v, T* wbuf, int tid, int B) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-    const int lane = tid & 31, wid = tid >> 5, nw = B >> 5;
-    __syncthreads();
-    if (lane == 0) wbuf[wid] = v;
-    __syncthreads();
-    T r = T(0);
-    if (wid == 0) {
-        r = lane < nw ? wbuf[lane] : T(0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xFFFFFFFFu, r, o);
-        if (lane == 0) wbuf[32] = r;
-    }
-    __syncthreads();
-    r = wbuf[32];
-    __syncthreads();
-    return r;
-}
+#define SRC(nd, p) ((p) ? (nd).reach_src1 : (nd).reach_src0)
 
 __device__ __forceinline__ DNode load_node(const DNode* p) {
     DNode d;
@@ -154,645 +109,679 @@ __device__ __forceinline__ DNode load_node(const DNode* p) {
     return d;
 }
 
-// Terminal values of both players at `node` into val (and val2 if given):
-// val[node*HS + off_q + h].  Reach of both players staged in sm_r.
-template <typename T>
-__device__ void eval_terminal(const SubDesc& sd, const DNode& nd, int node, const TabView& tv,
-                              const T* reach, T* val, T* val2, int HS, int semantics, T* sm_r, T* sm_x,
-                              T* wbuf, int tid, int B) {
-    const int H[2] = {sd.H0, sd.H1};
-    const int Hp[2] = {sd.Hp0, sd.Hp1};
-    const int off[2] = {0, sd.Hp0};
-    const int src[2] = {nd.reach_src0, nd.reach_src1};
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-        const T* r = reach + (size_t)src[p] * HS + OFF(p);
-        T* d = sm_r + (p ? H[0] : 0);
-        for (int j = tid; j < H[p]; j += B) d[j] = r[j];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int o = 1 - q, Ho = H[o];
-        const int base = q ? 3 * H[1] : 0;
-        const T* ro = sm_r + (o ? H[0] : 0);
-        const uint16_t* so = tv.sorted[o];
-        const uint16_t* co = tv.cl[o];
-        for (int i = tid; i < Ho; i += B) sm_x[base + i] = ro[so[i]];
-        for (int e = tid; e < 2 * Ho; e += B) sm_x[base + Ho + e] = ro[co[e]];
-    }
-    __syncthreads();
-    block_scan_excl<T>(sm_x, 3 * (H[0] + H[1]), wbuf, tid, B);
-    const bool fold = nd.type == MTT_NODE_FOLD;
-    const int winner = (nd.wmask == 1) ? 0 : 1;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int o = 1 - q, Ho = H[o];
-        const T* E = sm_x + (q ? 3 * H[1] : 0);
-        const T e0 = E[0];
-        const T Tt = E[Ho] - e0;
-        const T* ro = sm_r + (o ? H[0] : 0);
-        const uint16_t* seg = tv.seg[o];
-        const Entry* ent = tv.ent[q];
-        const T cq = (T)(q ? nd.c1 : nd.c0);
-        const T pot = (T)nd.pot;
-        const T gain = pot - cq, loss = -cq, tie = T(0.5) * pot - cq;
-        const T payoff = (q == winner) ? gain : loss;
-        T* out = val + (size_t)node * HS + off[q];
-        T* out2 = val2 ? val2 + (size_t)node * HS + off[q] : nullptr;
-        for (int h = tid; h < Hp[q]; h += B) {
-            T v = T(0);
-            if (h < H[q]) {
-                const Entry et = ent[h];
-                if (et.lt != 0xFFFFu) {
-                    const int s1 = Ho + seg[et.c1], s2 = Ho + seg[et.c2];
-                    const T b1 = E[s1], b2 = E[s2];
-                    const T C1 = E[Ho + seg[et.c1 + 1]] - b1, C2 = E[Ho + seg[et.c2 + 1]] - b2;
-                    const T ps = et.same >= 0 ? ro[et.same] : T(0);
-                    if (fold) {
-                        const T M = semantics ? Tt : (Tt - C1 - C2 + ps);
-                        v = payoff * M;
-                    } else {
-                        const T W = (E[et.lt] - e0) - (E[s1 + et.ltc1] - b1) - (E[s2 + et.ltc2] - b2);
-                        const T LE = (E[et.le] - e0) - (E[s1 + et.lec1] - b1) - (E[s2 + et.lec2] - b2);
-                        const T Ti = LE - W + ps;
-                        if (!semantics) {
-                            const T L = Tt - C1 - C2 - LE;
-                            v = gain * W + tie * Ti + loss * L;
-                        } else {
-                            const T Lr = Tt - W - Ti;   // blocked pairs count as P0 losses
-                            v = (q == 0) ? (gain * W + tie * Ti + loss * Lr) : (gain * Lr + tie * Ti + loss * W);
-                        }
-                    }
-                }
-            }
-            out[h] = v;
-            if (out2) out2[h] = v;
-        }
-    }
-    __syncthreads();
-}
-
 __device__ __forceinline__ uint64_t hand_mask(uint16_t hc) {
     return hc == 0xFFFFu ? 0ull : ((1ull << (hc & 0xFF)) | (1ull << (hc >> 8)));
 }
 
 template <typename T>
-__device__ __forceinline__ T blocked_zero(uint16_t hc, int card, T v) {
-    return (hand_mask(hc) >> card) & 1ull ? T(0) : v;
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
 }
 
-// ------------------------------------------------------------------ solve
-__device__ void solve_one(const BatchDev& a, const SubDesc& sd, uint8_t* smem, int tid, int B) {
-    const int nn = sd.n_nodes;
-    const int HS = sd.Hp0 + sd.Hp1, HS4 = HS >> 2;
-    float* reach = a.arena + sd.arena_base;
-    float* cfv = reach + (size_t)nn * HS;
-    const DNode* nodes = a.nodes + sd.node_base;
-    const uint16_t* hc = a.hcards + sd.hcard_base;
-    const int Hsum = sd.H0 + sd.H1;
-    float* sm_r = reinterpret_cast<float*>(smem);
-    float* sm_x = sm_r + ((Hsum + 3) & ~3);
-    float* wbuf = sm_x + ((3 * Hsum + 1 + 3) & ~3);
-    const float div = (float)(a.semantics ? sd.n_live - 2 : sd.n_live - 4);
+// ------------------------------------------------------------- terminals
+struct TermInfo {
+    int H[2], Hp[2];
+    float pot, c[2];
+    int type, wmask;
+};
 
-    // zero regrets and strategy sums, load root reach
+__device__ __forceinline__ TermInfo term_info(const SubDesc& sd, const DNode& nd) {
+    TermInfo t;
+    t.H[0] = sd.H0; t.H[1] = sd.H1; t.Hp[0] = sd.Hp0; t.Hp[1] = sd.Hp1;
+    t.pot = nd.pot; t.c[0] = nd.c0; t.c[1] = nd.c1;
+    t.type = nd.type; t.wmask = nd.wmask;
+    return t;
+}
+
+// Shared scratch of one terminal CTA, in elements of the arithmetic type.
+__host__ __device__ constexpr int term_scratch(int max_h) { return 4 * max_h + 96; }
+constexpr int TT = 128;   // threads per terminal CTA (fixed: results never depend on it changing)
+
+template <typename TA>
+__device__ __forceinline__ TA cta_sum(TA v, TA* wb, int tid) {
+    v = warp_sum(v);
+    if ((tid & 31) == 0) wb[tid >> 5] = v;
+    __syncthreads();
+    TA t = TA(0);
+#pragma unroll
+    for (int k = 0; k < TT / 32; ++k) t += wb[k];
+    __syncthreads();
+    return t;
+}
+
+// Values of player q at a terminal against opponent reach `ro` (H_o entries),
+// written to out[0..Hp_q) (and out2), by one CTA of TT threads.  TI: stored
+// reach type, TA: arithmetic type of the scan and differences, TO: stored
+// value type.  The solver keeps reach and values in FP32 but scans in FP64:
+// win/tie/loss masses are differences of prefix sums, and a value that is
+// exactly zero (all of the opponent's remaining mass blocked by the hand's
+// cards) must come out as zero to the precision the regret-matching
+// threshold (1e-7) can see.  X: the CTA's shared scratch (term_scratch
+// elements), wb: 8 elements.
+template <typename TI, typename TA, typename TO, bool STAGED = false>
+__device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const TI* __restrict__ ro,
+                             TO* __restrict__ out, TO* __restrict__ out2, TA* X, TA* wb, int semantics, int tid) {
+    const int o = 1 - q;
+    const int Ho = ti.H[o], Hq = ti.H[q], Hpq = ti.Hp[q];
+    const uint16_t* co = tv.cl[o];
+    const uint16_t* seg = tv.seg[o];
+    const Entry* ent = tv.ent[q];
+    const TA cq = (TA)ti.c[q];
+    const TA pot = (TA)ti.pot;
+    const TA gain = pot - cq, loss = -cq, tie = TA(0.5) * pot - cq;
+    // opponent reach: already in shared memory (STAGED), else staged here with coalesced loads
+    TA* Rd = X;
+    TA* Xs = STAGED ? X : X + Ho + 8;   // scan region (3*Ho + 1) / fold: per-card order + card sums
+    if (!STAGED) {
+#pragma unroll 4
+        for (int j = tid; j < Ho; j += TT) Rd[j] = (TA)ro[j];
+        __syncthreads();
+    }
+    auto Rs = [&](int j) -> TA { return STAGED ? (TA)ro[j] : Rd[j]; };
+    if (ti.type == MTT_NODE_FOLD) {
+        const int winner = (ti.wmask == 1) ? 0 : 1;
+        const TA payoff = (q == winner) ? gain : loss;
+        TA part = TA(0);
+        for (int j = tid; j < Ho; j += TT) part += Rs(j);
+        const TA tot = cta_sum(part, wb, tid);
+        TA* Cs = Xs + 2 * Ho + 8;
+#pragma unroll 4
+        for (int e = tid; e < 2 * Ho; e += TT) Xs[e] = Rs(co[e]);
+        __syncthreads();
+        for (int c = tid; c < 52; c += TT) {
+            TA sm = TA(0);
+            for (int e = seg[c]; e < seg[c + 1]; ++e) sm += Xs[e];
+            Cs[c] = sm;
+        }
+        __syncthreads();
+        for (int h = tid; h < Hpq; h += TT) {
+            TA v = TA(0);
+            if (h < Hq) {
+                const Entry et = ent[h];
+                if (et.lt != 0xFFFFu) {
+                    const TA ps = et.same >= 0 ? Rs(et.same) : TA(0);
+                    const TA M = semantics ? tot : (tot - Cs[et.c1] - Cs[et.c2] + ps);
+                    v = payoff * M;
+                }
+            }
+            out[h] = (TO)v;
+            if (out2) out2[h] = (TO)v;
+        }
+        __syncthreads();
+        return;
+    }
+    // showdown: Xs = [reach in rank order | reach in per-card rank order], exclusive scan
+    const uint16_t* so = tv.sorted[o];
+    const int N = 3 * Ho;
+#pragma unroll 4
+    for (int k = tid; k < N; k += TT) Xs[k] = Rs(k < Ho ? so[k] : co[k - Ho]);
+    __syncthreads();
+    const int C = ((N + TT - 1) / TT) | 1;   // odd chunk: conflict-free strides
+    const int s0 = min(tid * C, N), s1 = min(s0 + C, N);
+    TA loc = TA(0);
+    for (int k = s0; k < s1; ++k) loc += Xs[k];
+    const int lane = tid & 31, wid = tid >> 5;
+    TA inc = loc;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const TA t = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+        if (lane >= off) inc += t;
+    }
+    TA run = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+    if (lane == 0) run = TA(0);
+    if (lane == 31) wb[wid] = inc;
+    __syncthreads();
+    TA base = TA(0), total = TA(0);
+#pragma unroll
+    for (int k = 0; k < TT / 32; ++k) {
+        if (k < wid) base += wb[k];
+        total += wb[k];
+    }
+    run += base;
+    for (int k = s0; k < s1; ++k) {
+        const TA v = Xs[k];
+        Xs[k] = run;
+        run += v;
+    }
+    if (tid == 0) Xs[N] = total;
+    __syncthreads();
+    const TA Tt = Xs[Ho];
+    for (int h = tid; h < Hpq; h += TT) {
+        TA v = TA(0);
+        if (h < Hq) {
+            const Entry et = ent[h];
+            if (et.lt != 0xFFFFu) {
+                const int s1c = Ho + seg[et.c1], s2c = Ho + seg[et.c2];
+                const TA b1 = Xs[s1c], b2 = Xs[s2c];
+                const TA C1 = Xs[Ho + seg[et.c1 + 1]] - b1, C2 = Xs[Ho + seg[et.c2 + 1]] - b2;
+ 
+                const TA ps = et.same >= 0 ? Rs(et.same) : TA(0);
+                const TA W = Xs[et.lt] - (Xs[s1c + et.ltc1] - b1) - (Xs[s2c + et.ltc2] - b2);
+                const TA LE = Xs[et.le] - (Xs[s1c + et.lec1] - b1) - (Xs[s2c + et.lec2] - b2);
+                const TA Ti = LE - W + ps;
+                if (!semantics) {
+                    const TA L = Tt - C1 - C2 - LE;
+                    v = gain * W + tie * Ti + loss * L;
+                } else {
+                    const TA Lr = Tt - W - Ti;   // blocked pairs count as P0 losses (honest:182-187)
+                    v = (q == 0) ? (gain * W + tie * Ti + loss * Lr) : (gain * Lr + tie * Ti + loss * W);
+                }
+            }
+        }
+        out[h] = (TO)v;
+        if (out2) out2[h] = (TO)v;
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------- solve kernels
+// Work items carry absolute offsets so a warp needs one load before it
+// streams: a sweep item is one node for one player, a warp loops over that
+// player's float4 hand groups.
+struct alignas(16) FwdItem {    // 64 B
+    long long reach_in;   // arena float offset of the acting player's reach at the node
+    long long child;      // arena float offset of child 0's part for that player
+    long long rows;       // R/S float offset of the node's first regret row
+    long long hc;         // hand-card offset of that player (chance items)
+    int h4;               // float4 groups of that player
+    int hs4;              // reach slot stride in float4
+    int na;
+    int flags;            // FI_REACH: write children's reach; FI_SUMS: add to S; FI_CHANCE
+    int first;            // global index of child 0 (chance items read the dealt cards)
+    int g0;               // first float4 group of this warp (lane l takes g0 + l)
+    int sub;              // subgame
+    int pad;
+};
+struct alignas(16) BwdItem {    // 64 B
+    long long child;      // arena float offset (CFV region) of child 0's part for player q
+    long long self;       // arena float offset (CFV region) of this node's part for q
+    long long rows;       // R float offset of the node's first row (update items)
+    long long hc;         // hand-card offset of q (chance items)
+    int h4;
+    int hs4;
+    int na;
+    int flags;            // BI_UPDATE: q acts here; BI_CHANCE; otherwise sum of children
+    int first;            // global index of child 0 (chance items)
+    float div;            // chance divisor
+    int g0;               // first float4 group of this warp
+    int sub;              // subgame
+};
+struct alignas(16) TermItem {   // 80 B
+    long long ro[2];      // arena offsets of each player's reach at the terminal
+    long long out[2];     // arena offsets (CFV region) of each player's values
+    long long tab;        // byte offset of the showdown table variant
+    float pot, c0, c1;
+    int type_wmask;       // type | wmask << 8
+    int H[2], Hp[2];
+    int sub;              // subgame
+    int pad[3];
+};
+static_assert(sizeof(FwdItem) == 64 && sizeof(BwdItem) == 64 && sizeof(TermItem) == 96, "item sizes");
+enum { FI_REACH = 1, FI_SUMS = 2, FI_CHANCE = 4 };
+enum { BI_UPDATE = 1, BI_CHANCE = 4 };
+
+__global__ void k_init(SolveDev a, int n_sub) {
+    const int s = blockIdx.x;
+    if (s == 0 && threadIdx.x == 0) { *a.iter = 1; *a.err = 0; }
+    if (s >= n_sub) return;
+    const SubDesc sd = a.desc[s];
+    const long long n0 = (long long)sd.rows0 * sd.Hp0 / 4, n1 = (long long)sd.rows1 * sd.Hp1 / 4;
+    float4* r0 = reinterpret_cast<float4*>(a.R + sd.rs_base0);
+    float4* r1 = reinterpret_cast<float4*>(a.R + sd.rs_base1);
+    float4* s0 = reinterpret_cast<float4*>(a.S + sd.rs_base0);
+    float4* s1 = reinterpret_cast<float4*>(a.S + sd.rs_base1);
+    for (long long i = threadIdx.x; i < n0; i += blockDim.x) { r0[i] = f4(0.f); s0[i] = f4(0.f); }
+    for (long long i = threadIdx.x; i < n1; i += blockDim.x) { r1[i] = f4(0.f); s1[i] = f4(0.f); }
+    const int HS4 = (sd.Hp0 + sd.Hp1) >> 2;
+    const float4* rg = reinterpret_cast<const float4*>(a.ranges + sd.range_base);
+    float4* rr = reinterpret_cast<float4*>(a.arena + sd.arena_base);
+    for (int i = threadIdx.x; i < HS4; i += blockDim.x) rr[i] = rg[i];
+}
+
+__global__ void k_next_iter(SolveDev a) {
+    if (threadIdx.x == 0) *a.iter += 1;
+}
+
+// Forward sweep of one level: regret matching, children's reach and/or
+// strategy sums (kernel_forward_sweep, honest_multistreet_solver.cu:88-126).
+__global__ void __launch_bounds__(256, 3) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const FwdItem it = items[w];
+    const float4* rp = reinterpret_cast<const float4*>(a.arena + it.reach_in);
+    float4* ch = reinterpret_cast<float4*>(a.arena + it.child);
+    const int A = it.na, H4 = it.h4, HS4 = it.hs4;
+    if (it.flags & FI_CHANCE) {
+        const uint16_t* hc = a.hcards + it.hc;
+        const int g = it.g0 + lane;
+        if (g < H4) {
+            const float4 r = rp[g];
+            const uint64_t m0 = hand_mask(hc[4 * g]), m1 = hand_mask(hc[4 * g + 1]);
+            const uint64_t m2 = hand_mask(hc[4 * g + 2]), m3 = hand_mask(hc[4 * g + 3]);
+            for (int k = 0; k < A; ++k) {
+                const int card = a.nodes[it.first + k].dealt;
+                float4 v = r;
+                if ((m0 >> card) & 1ull) v.x = 0.f;
+                if ((m1 >> card) & 1ull) v.y = 0.f;
+                if ((m2 >> card) & 1ull) v.z = 0.f;
+                if ((m3 >> card) & 1ull) v.w = 0.f;
+                ch[(size_t)k * HS4 + g] = v;
+            }
+        }
+        return;
+    }
+    const bool dr = it.flags & FI_REACH, ds = it.flags & FI_SUMS;
+    const float4* Rb = reinterpret_cast<const float4*>(a.R + it.rows);
+    float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
+    const float invA = __fdiv_rn(1.0f, (float)A);
+    float w_lin = 0.f, dstr = 0.f;
+    if (ds) {
+        const float4 tb = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (*a.iter - 1));
+        w_lin = tb.x;
+        dstr = tb.w;
+    }
+    const bool dcfr = a.algo == MTT_ALGO_DCFR;
+    // Regret rows are read twice (sum, then strategy); the second read hits
+    // L1, which keeps registers low.
+    const int g = it.g0 + lane;
+    if (g < H4) {
+        const float4 r = rp[g];
+        float4 sum = f4(0.f);
+        for (int k = 0; k < A; ++k) sum = add4(sum, max04(Rb[(size_t)k * H4 + g]));
+        const float4 wr = mul4(r, f4(w_lin));
+        for (int k = 0; k < A; ++k) {
+            const float4 sg = rm4(max04(Rb[(size_t)k * H4 + g]), sum, invA);
+            if (dr) ch[(size_t)k * HS4 + g] = mul4(r, sg);
+            if (ds) {
+                float4 sv = Sb[(size_t)k * H4 + g];
+                sv = dcfr ? fma4(r, sg, mul4(sv, f4(dstr))) : fma4(wr, sg, sv);
+                Sb[(size_t)k * H4 + g] = sv;
+            }
+        }
+    }
+}
+
+// Shared memory of one staged terminal direction: the opponent's reach
+// (FP32), the opponent's index block, this player's entry block and the FP64
+// scan region.
+__host__ __device__ inline int term_stage_bytes(int Hpo, int Ho, int Hq) {
+    // FP64 region: showdown scan 3*Ho + 1, fold per-card order 2*Ho + card sums at 2*Ho + 8 .. + 52
+    const int xd = (3 * Ho + 8) > (2 * Ho + 64) ? (3 * Ho + 8) : (2 * Ho + 64);
+    return 4 * Hpo + tab_idx_bytes(Ho) + tab_ent_bytes(Hq) + 8 * xd + 64;
+}
+
+// Terminal values of the updated players, one CTA per terminal
+// (kernel_evaluate_terminals, honest_multistreet_solver.cu:128-196).  Thread 0
+// stages the opponent's reach, the opponent's rank/card index block and this
+// player's entry block into shared memory with three 1-D bulk copies on one
+// mbarrier; the CTA then works from shared memory only.
+__global__ void __launch_bounds__(TT) k_term(SolveDev a, const TermItem* __restrict__ items, int n, int upd) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ double wb[8];
+    const int w = blockIdx.x, tid = threadIdx.x;
+    if (w >= n) return;
+    const TermItem it = items[w];
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t parity = 0u;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (!((upd >> q) & 1)) continue;
+        const int o = 1 - q;
+        const int Ho = it.H[o], Hpo = it.Hp[o], Hq = it.H[q];
+        const uint32_t rb = 4u * (uint32_t)Hpo, ib = (uint32_t)tab_idx_bytes(Ho), eb = (uint32_t)tab_ent_bytes(Hq);
+        float* Ro = reinterpret_cast<float*>(smem);
+        uint8_t* Ib = smem + rb;
+        uint8_t* Eb = Ib + ib;
+        double* X = reinterpret_cast<double*>(Eb + eb);   // rb, ib, eb are multiples of 16
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&bar, rb + ib + eb);
+            bulk_g2s(Ro, a.arena + it.ro[o], rb, &bar);
+            bulk_g2s(Ib, a.tabs + it.tab + tab_idx_off(o, it.H[0]), ib, &bar);
+            bulk_g2s(Eb, a.tabs + it.tab + tab_ent_off(q, it.H[0], it.H[1]), eb, &bar);
+        }
+        const bool ok = mbar_wait_bounded(&bar, parity);
+        parity ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(a.err, 1);
+            return;
+        }
+        TabView tv;
+        tab_idx_view(Ib, Ho, &tv.sorted[o], &tv.cl[o], &tv.seg[o]);
+        tv.ent[q] = reinterpret_cast<const Entry*>(Eb);
+        TermInfo ti;
+        ti.H[0] = it.H[0]; ti.H[1] = it.H[1]; ti.Hp[0] = it.Hp[0]; ti.Hp[1] = it.Hp[1];
+        ti.pot = it.pot; ti.c[0] = it.c0; ti.c[1] = it.c1;
+        ti.type = it.type_wmask & 0xFF; ti.wmask = (it.type_wmask >> 8) & 0xFF;
+        cta_terminal<float, double, float, true>(ti, tv, q, Ro, a.arena + it.out[q], nullptr, X, wb, a.semantics, tid);
+    }
+}
+
+// Backward sweep of one level for the updated players: counterfactual values
+// and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
+__global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const BwdItem it = items[w];
+    const float4* qc = reinterpret_cast<const float4*>(a.arena + it.child);
+    float4* out = reinterpret_cast<float4*>(a.arena + it.self);
+    const int A = it.na, H4 = it.h4, HS4 = it.hs4;
+    if (it.flags & BI_CHANCE) {
+        const uint16_t* hc = a.hcards + it.hc;
+        const float dv = a.semantics ? it.div + 2.0f : it.div;   // (N-2) in the reference's semantics
+        const int g = it.g0 + lane;
+        if (g < H4) {
+            const uint64_t m0 = hand_mask(hc[4 * g]), m1 = hand_mask(hc[4 * g + 1]);
+            const uint64_t m2 = hand_mask(hc[4 * g + 2]), m3 = hand_mask(hc[4 * g + 3]);
+            float4 acc = f4(0.f);
+            for (int k = 0; k < A; ++k) {
+                const int card = a.nodes[it.first + k].dealt;
+                const float4 cv = qc[(size_t)k * HS4 + g];
+                if (!((m0 >> card) & 1ull)) acc.x = __fadd_rn(acc.x, cv.x);
+                if (!((m1 >> card) & 1ull)) acc.y = __fadd_rn(acc.y, cv.y);
+                if (!((m2 >> card) & 1ull)) acc.z = __fadd_rn(acc.z, cv.z);
+                if (!((m3 >> card) & 1ull)) acc.w = __fadd_rn(acc.w, cv.w);
+            }
+            out[g] = make_float4(__fdiv_rn(acc.x, dv), __fdiv_rn(acc.y, dv), __fdiv_rn(acc.z, dv), __fdiv_rn(acc.w, dv));
+        }
+        return;
+    }
+    const int g = it.g0 + lane;
+    if (g >= H4) return;
+    if (!(it.flags & BI_UPDATE)) {
+        {
+            float4 so = f4(0.f);
+            for (int k = 0; k < A; ++k) so = add4(so, qc[(size_t)k * HS4 + g]);
+            out[g] = so;
+        }
+        return;
+    }
+    const float invA = __fdiv_rn(1.0f, (float)A);
+    float4* Rb = reinterpret_cast<float4*>(a.R + it.rows);
+    float dpos = 0.f, dneg = 0.f;
+    const bool dcfr = a.algo == MTT_ALGO_DCFR;
+    if (dcfr) {
+        const float4 tb = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (*a.iter - 1));
+        dpos = tb.y;
+        dneg = tb.z;
+    }
+    // Rows and child values are re-read (L1 hits) instead of held in registers.
     {
-        const long long n0 = (long long)sd.rows0 * sd.Hp0 / 4, n1 = (long long)sd.rows1 * sd.Hp1 / 4;
-        float4* r0 = reinterpret_cast<float4*>(RP(0));
-        float4* r1 = reinterpret_cast<float4*>(RP(1));
-        float4* s0 = reinterpret_cast<float4*>(SP(0));
-        float4* s1 = reinterpret_cast<float4*>(SP(1));
-        for (long long i = tid; i < n0; i += B) { r0[i] = f4(0.f); s0[i] = f4(0.f); }
-        for (long long i = tid; i < n1; i += B) { r1[i] = f4(0.f); s1[i] = f4(0.f); }
-        const float4* rg = reinterpret_cast<const float4*>(a.ranges + sd.range_base);
-        float4* rr = reinterpret_cast<float4*>(reach);
-        for (int i = tid; i < HS4; i += B) rr[i] = rg[i];
-    }
-    __syncthreads();
-
-    for (int t = 1; t <= a.iters; ++t) {
-        const float4 it = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (t - 1));
-        const float w = it.x, dpos = it.y, dneg = it.z, dstr = it.w;
-        // ---------------- forward: regret matching, reach, strategy sums
-        for (int n = 0; n < nn; ++n) {
-            const DNode nd = load_node(nodes + n);
-            if (nd.type == MTT_NODE_DECISION) {
-                const int p = nd.player, A = nd.na, H4 = HP(p) >> 2;
-                const float invA = __fdiv_rn(1.0f, (float)A);
-                const float4* rp = reinterpret_cast<const float4*>(reach + (size_t)(p ? nd.reach_src1 : nd.reach_src0) * HS + OFF(p));
-                float4* ch = reinterpret_cast<float4*>(reach + (size_t)nd.first * HS + OFF(p));
-                const float4* Rb = reinterpret_cast<const float4*>(RP(p) + (size_t)nd.row * HP(p));
-                float4* Sb = reinterpret_cast<float4*>(SP(p) + (size_t)nd.row * HP(p));
-                for (int g = tid; g < H4; g += B) {
-                    const float4 r = rp[g];
-                    float4 pos[MAXA];
-                    float4 sum = f4(0.f);
-#pragma unroll
-                    for (int k = 0; k < MAXA; ++k)
-                        if (k < A) { pos[k] = max04(Rb[(size_t)k * H4 + g]); sum = add4(sum, pos[k]); }
-                    const float4 wr = mul4(r, f4(w));
-#pragma unroll
-                    for (int k = 0; k < MAXA; ++k)
-                        if (k < A) {
-                            const float4 sg = rm4(pos[k], sum, invA);
-                            ch[(size_t)k * HS4 + g] = mul4(r, sg);
-                            float4 sv = Sb[(size_t)k * H4 + g];
-                            sv = a.algo == MTT_ALGO_DCFR ? fma4(r, sg, mul4(sv, f4(dstr))) : fma4(wr, sg, sv);
-                            Sb[(size_t)k * H4 + g] = sv;
-                        }
-                }
-            } else if (nd.type == MTT_NODE_CHANCE) {
-                for (int k = 0; k < nd.na; ++k) {
-                    const int card = nodes[nd.first + k].dealt;
-#pragma unroll
-                    for (int p = 0; p < 2; ++p) {
-                        const int H4 = HP(p) >> 2;
-                        const float4* rp = reinterpret_cast<const float4*>(reach + (size_t)(p ? nd.reach_src1 : nd.reach_src0) * HS + OFF(p));
-                        float4* ch = reinterpret_cast<float4*>(reach + (size_t)(nd.first + k) * HS + OFF(p));
-                        const uint16_t* hcp = hc + OFF(p);
-                        for (int g = tid; g < H4; g += B) {
-                            float4 r = rp[g];
-                            r.x = blocked_zero(hcp[4 * g + 0], card, r.x);
-                            r.y = blocked_zero(hcp[4 * g + 1], card, r.y);
-                            r.z = blocked_zero(hcp[4 * g + 2], card, r.z);
-                            r.w = blocked_zero(hcp[4 * g + 3], card, r.w);
-                            ch[g] = r;
-                        }
-                    }
-                }
+        float4 sum = f4(0.f);
+        for (int k = 0; k < A; ++k) sum = add4(sum, max04(Rb[(size_t)k * H4 + g]));
+        float4 v = f4(0.f);
+        for (int k = 0; k < A; ++k)
+            v = fma4(rm4(max04(Rb[(size_t)k * H4 + g]), sum, invA), qc[(size_t)k * HS4 + g], v);
+        out[g] = v;
+        for (int k = 0; k < A; ++k) {
+            const float4 rk = Rb[(size_t)k * H4 + g];
+            const float4 qk = qc[(size_t)k * HS4 + g];
+            float4 nr;
+            if (dcfr) {
+                nr.x = dcfr1(rk.x, __fsub_rn(qk.x, v.x), dpos, dneg);
+                nr.y = dcfr1(rk.y, __fsub_rn(qk.y, v.y), dpos, dneg);
+                nr.z = dcfr1(rk.z, __fsub_rn(qk.z, v.z), dpos, dneg);
+                nr.w = dcfr1(rk.w, __fsub_rn(qk.w, v.w), dpos, dneg);
+            } else {
+                nr.x = cfrplus1(rk.x, __fsub_rn(qk.x, v.x));
+                nr.y = cfrplus1(rk.y, __fsub_rn(qk.y, v.y));
+                nr.z = cfrplus1(rk.z, __fsub_rn(qk.z, v.z));
+                nr.w = cfrplus1(rk.w, __fsub_rn(qk.w, v.w));
             }
+            Rb[(size_t)k * H4 + g] = nr;
         }
-        __syncthreads();
-        // ---------------- terminals
-        for (int n = 0; n < nn; ++n) {
-            const DNode nd = load_node(nodes + n);
-            if (nd.type != MTT_NODE_FOLD && nd.type != MTT_NODE_SHOWDOWN) continue;
-            const int v = tab_variant(sd.river, nd.dealt);
-            const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)v * sd.tab_vsize, sd.H0, sd.H1);
-            eval_terminal<float>(sd, nd, n, tv, reach, cfv, nullptr, HS, a.semantics, sm_r, sm_x, wbuf, tid, B);
-        }
-        // ---------------- backward: values and regrets
-        for (int n = nn - 1; n >= 0; --n) {
-            const DNode nd = load_node(nodes + n);
-            if (nd.type == MTT_NODE_DECISION) {
-                const int p = nd.player, o = 1 - p, A = nd.na;
-                const int H4 = HP(p) >> 2, H4o = HP(o) >> 2;
-                const float invA = __fdiv_rn(1.0f, (float)A);
-                float4* Rb = reinterpret_cast<float4*>(RP(p) + (size_t)nd.row * HP(p));
-                const float4* qc = reinterpret_cast<const float4*>(cfv + (size_t)nd.first * HS + OFF(p));
-                float4* outp = reinterpret_cast<float4*>(cfv + (size_t)n * HS + OFF(p));
-                for (int g = tid; g < H4; g += B) {
-                    // only the regrets stay in registers; the child values
-                    // are re-read (an L1 hit) for the update
-                    float4 rr[MAXA];
-                    float4 sum = f4(0.f);
-#pragma unroll
-                    for (int k = 0; k < MAXA; ++k)
-                        if (k < A) {
-                            rr[k] = Rb[(size_t)k * H4 + g];
-                            sum = add4(sum, max04(rr[k]));
-                        }
-                    float4 v = f4(0.f);
-#pragma unroll
-                    for (int k = 0; k < MAXA; ++k)
-                        if (k < A) v = fma4(rm4(max04(rr[k]), sum, invA), qc[(size_t)k * HS4 + g], v);
-                    outp[g] = v;
-#pragma unroll
-                    for (int k = 0; k < MAXA; ++k)
-                        if (k < A) {
-                            const float4 qk = qc[(size_t)k * HS4 + g];
-                            float4 nr;
-                            if (a.algo == MTT_ALGO_DCFR) {
-                                nr.x = dcfr1(rr[k].x, __fsub_rn(qk.x, v.x), dpos, dneg);
-                                nr.y = dcfr1(rr[k].y, __fsub_rn(qk.y, v.y), dpos, dneg);
-                                nr.z = dcfr1(rr[k].z, __fsub_rn(qk.z, v.z), dpos, dneg);
-                                nr.w = dcfr1(rr[k].w, __fsub_rn(qk.w, v.w), dpos, dneg);
-                            } else {
-                                nr.x = cfrplus1(rr[k].x, __fsub_rn(qk.x, v.x));
-                                nr.y = cfrplus1(rr[k].y, __fsub_rn(qk.y, v.y));
-                                nr.z = cfrplus1(rr[k].z, __fsub_rn(qk.z, v.z));
-                                nr.w = cfrplus1(rr[k].w, __fsub_rn(qk.w, v.w));
-                            }
-                            Rb[(size_t)k * H4 + g] = nr;
-                        }
-                }
-                const float4* oc = reinterpret_cast<const float4*>(cfv + (size_t)nd.first * HS + OFF(o));
-                float4* outo = reinterpret_cast<float4*>(cfv + (size_t)n * HS + OFF(o));
-                for (int g = tid; g < H4o; g += B) {
-                    float4 so = f4(0.f);
-                    for (int k = 0; k < A; ++k) so = add4(so, oc[(size_t)k * HS4 + g]);
-                    outo[g] = so;
-                }
-            } else if (nd.type == MTT_NODE_CHANCE) {
-#pragma unroll
-                for (int p = 0; p < 2; ++p) {
-                    const int H4 = HP(p) >> 2;
-                    const uint16_t* hcp = hc + OFF(p);
-                    float4* outp = reinterpret_cast<float4*>(cfv + (size_t)n * HS + OFF(p));
-                    for (int g = tid; g < H4; g += B) {
-                        const uint64_t m0 = hand_mask(hcp[4 * g]), m1 = hand_mask(hcp[4 * g + 1]);
-                        const uint64_t m2 = hand_mask(hcp[4 * g + 2]), m3 = hand_mask(hcp[4 * g + 3]);
-                        float4 acc = f4(0.f);
-                        for (int k = 0; k < nd.na; ++k) {
-                            const int card = nodes[nd.first + k].dealt;
-                            const float4 cv = reinterpret_cast<const float4*>(cfv + (size_t)(nd.first + k) * HS + OFF(p))[g];
-                            if (!((m0 >> card) & 1ull)) acc.x = __fadd_rn(acc.x, cv.x);
-                            if (!((m1 >> card) & 1ull)) acc.y = __fadd_rn(acc.y, cv.y);
-                            if (!((m2 >> card) & 1ull)) acc.z = __fadd_rn(acc.z, cv.z);
-                            if (!((m3 >> card) & 1ull)) acc.w = __fadd_rn(acc.w, cv.w);
-                        }
-                        outp[g] = make_float4(__fdiv_rn(acc.x, div), __fdiv_rn(acc.y, div), __fdiv_rn(acc.z, div),
-                                              __fdiv_rn(acc.w, div));
-                    }
-                }
-            }
-        }
-        // The next forward sweep touches only this thread's own hands and
-        // the terminal phase starts behind a barrier, so none is needed here.
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(256, 2) k_batch_solve(BatchDev a) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    __shared__ int s_item;
-    const int tid = threadIdx.x, B = blockDim.x;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.queue, 1);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= a.n_sub) return;
-        const int s = a.order ? a.order[item] : item;
-        const SubDesc sd = a.desc[s];
-        solve_one(a, sd, smem, tid, B);
     }
 }
 
 // ------------------------------------------------------------- FP64 best response
-__device__ void br_one(const BatchDev& a, const SubDesc& sd, int s, uint8_t* smem, int tid, int B) {
-    const int nn = sd.n_nodes;
+// darena per subgame: reach | br | ev, each (n_nodes + 1) * HS doubles; the
+// extra slot holds the compatible-mass values of the root.
+__device__ __forceinline__ double avg_sigma(const float* Sb, int Hp, int k, int A, int h) {
+    double sum = 0.0;
+    for (int j = 0; j < A; ++j) sum += (double)Sb[(size_t)j * Hp + h];
+    return sum > 0.0 ? (double)Sb[(size_t)k * Hp + h] / sum : 1.0 / (double)A;
+}
+
+__global__ void k_br_init(SolveDev a, const int* __restrict__ subs, int n_sub) {
+    if ((int)blockIdx.x >= n_sub) return;
+    const int s = subs[blockIdx.x];
+    const SubDesc sd = a.desc[s];
     const int HS = sd.Hp0 + sd.Hp1;
+    double* reach = a.darena + sd.darena_base;
+    for (int i = threadIdx.x; i < HS; i += blockDim.x) reach[i] = (double)a.ranges[sd.range_base + i];
+}
+
+__global__ void __launch_bounds__(256) k_br_fwd(SolveDev a, const Task* __restrict__ tasks, int ntasks) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= ntasks) return;
+    const Task tk = tasks[w];
+    const SubDesc& sd = a.desc[tk.sub];
+    const DNode nd = load_node(a.nodes + tk.node);
+    const int g = tk.g0 + lane;
+    const int HS = sd.Hp0 + sd.Hp1;
+    double* reach = a.darena + sd.darena_base;
+    if (nd.type == MTT_NODE_DECISION) {
+        const int p = nd.player, A = nd.na, Hpp = HP(p);
+        if (4 * g >= Hpp) return;
+        const float* Sb = a.S + (p ? sd.rs_base1 : sd.rs_base0) + (size_t)nd.row * Hpp;
+        const double* rp = reach + (size_t)SRC(nd, p) * HS + OFF(p);
+        for (int i = 0; i < 4; ++i) {
+            const int h = 4 * g + i;
+            const double r = rp[h];
+            for (int k = 0; k < A; ++k)
+                reach[(size_t)(nd.first + k) * HS + OFF(p) + h] = r * avg_sigma(Sb, Hpp, k, A, h);
+        }
+    } else if (nd.type == MTT_NODE_CHANCE) {
+        const DNode* nodes = a.nodes + sd.node_base;
+        const uint16_t* hc = a.hcards + sd.hcard_base;
+        for (int p = 0; p < 2; ++p) {
+            if (4 * g >= HP(p)) continue;
+            const double* rp = reach + (size_t)SRC(nd, p) * HS + OFF(p);
+            for (int k = 0; k < nd.na; ++k) {
+                const int card = nodes[nd.first + k].dealt;
+                for (int i = 0; i < 4; ++i) {
+                    const int h = 4 * g + i;
+                    reach[(size_t)(nd.first + k) * HS + OFF(p) + h] =
+                        ((hand_mask(hc[OFF(p) + h]) >> card) & 1ull) ? 0.0 : rp[h];
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TT) k_br_term(SolveDev a, const int2* __restrict__ terms, int nterms) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ double wb[8];
+    const int w = blockIdx.x;
+    if (w >= nterms) return;
+    const int2 tm = terms[w];
+    const SubDesc& sd = a.desc[tm.y];
+    const DNode nd = load_node(a.nodes + tm.x);
+    const int nl = tm.x - (int)sd.node_base;
+    const int HS = sd.Hp0 + sd.Hp1;
+    const size_t reg = (size_t)(sd.n_nodes + 1) * HS;
+    double* reach = a.darena + sd.darena_base;
+    double* br = reach + reg;
+    double* ev = br + reg;
+    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)tab_variant(sd.river, nd.dealt) * sd.tab_vsize,
+                                sd.H0, sd.H1);
+    double* X = reinterpret_cast<double*>(smem);
+    for (int q = 0; q < 2; ++q) {
+        const int o = 1 - q;
+        cta_terminal<double, double, double>(term_info(sd, nd), tv, q, reach + (size_t)SRC(nd, o) * HS + OFF(o),
+                                             br + (size_t)nl * HS + OFF(q), ev + (size_t)nl * HS + OFF(q), X, wb,
+                                             MTT_SEM_CORRECT, threadIdx.x);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_br_bwd(SolveDev a, const Task* __restrict__ tasks, int ntasks) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= ntasks) return;
+    const Task tk = tasks[w];
+    const SubDesc& sd = a.desc[tk.sub];
+    const DNode nd = load_node(a.nodes + tk.node);
+    const int nl = tk.node - (int)sd.node_base;
+    const int g = tk.g0 + lane;
+    const int HS = sd.Hp0 + sd.Hp1;
+    const size_t reg = (size_t)(sd.n_nodes + 1) * HS;
+    double* br = a.darena + sd.darena_base + reg;
+    double* ev = br + reg;
+    if (nd.type == MTT_NODE_DECISION) {
+        const int p = nd.player, A = nd.na;
+        for (int q = 0; q < 2; ++q) {
+            const int Hpq = HP(q);
+            if (4 * g >= Hpq) continue;
+            const float* Sb = a.S + (p ? sd.rs_base1 : sd.rs_base0) + (size_t)nd.row * HP(p);
+            for (int i = 0; i < 4; ++i) {
+                const int h = 4 * g + i;
+                double b = q == p ? -1e300 : 0.0, e = 0.0;
+                for (int k = 0; k < A; ++k) {
+                    const size_t c = (size_t)(nd.first + k) * HS + OFF(q) + h;
+                    if (q == p) {
+                        b = fmax(b, br[c]);
+                        e += avg_sigma(Sb, HP(p), k, A, h) * ev[c];
+                    } else {
+                        b += br[c];
+                        e += ev[c];
+                    }
+                }
+                br[(size_t)nl * HS + OFF(q) + h] = b;
+                ev[(size_t)nl * HS + OFF(q) + h] = e;
+            }
+        }
+    } else if (nd.type == MTT_NODE_CHANCE) {
+        const DNode* nodes = a.nodes + sd.node_base;
+        const uint16_t* hc = a.hcards + sd.hcard_base;
+        const double div = (double)(sd.n_live - 4);
+        for (int q = 0; q < 2; ++q) {
+            if (4 * g >= HP(q)) continue;
+            for (int i = 0; i < 4; ++i) {
+                const int h = 4 * g + i;
+                const uint64_t m = hand_mask(hc[OFF(q) + h]);
+                double sb = 0.0, se = 0.0;
+                for (int k = 0; k < nd.na; ++k) {
+                    const int card = nodes[nd.first + k].dealt;
+                    if ((m >> card) & 1ull) continue;
+                    const size_t c = (size_t)(nd.first + k) * HS + OFF(q) + h;
+                    sb += br[c];
+                    se += ev[c];
+                }
+                br[(size_t)nl * HS + OFF(q) + h] = sb / div;
+                ev[(size_t)nl * HS + OFF(q) + h] = se / div;
+            }
+        }
+    }
+}
+
+// One CTA per subgame: compatible range mass and the four root values.
+__global__ void __launch_bounds__(TT) k_br_final(SolveDev a, const int* __restrict__ subs, int n_sub) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ double wb[8];
+    const int tid = threadIdx.x;
+    if ((int)blockIdx.x >= n_sub) return;
+    const int s = subs[blockIdx.x];
+    const SubDesc& sd = a.desc[s];
+    const int HS = sd.Hp0 + sd.Hp1;
+    const int nn = sd.n_nodes;
     const size_t reg = (size_t)(nn + 1) * HS;
     double* reach = a.darena + sd.darena_base;
     double* br = reach + reg;
     double* ev = br + reg;
-    const DNode* nodes = a.nodes + sd.node_base;
-    const uint16_t* hc = a.hcards + sd.hcard_base;
-    const int Hsum = sd.H0 + sd.H1;
-    double* sm_r = reinterpret_cast<double*>(smem);
-    double* sm_x = sm_r + Hsum + 1;
-    double* wbuf = sm_x + 3 * Hsum + 2;
-    const double div = (double)(sd.n_live - 4);
-
-    for (int i = tid; i < HS; i += B) reach[i] = (double)a.ranges[sd.range_base + i];
-    __syncthreads();
-    // forward with the average strategies
-    for (int n = 0; n < nn; ++n) {
-        const DNode nd = load_node(nodes + n);
-        if (nd.type == MTT_NODE_DECISION) {
-            const int p = nd.player, A = nd.na;
-            const double* rp = reach + (size_t)(p ? nd.reach_src1 : nd.reach_src0) * HS + OFF(p);
-            const float* Sb = SP(p) + (size_t)nd.row * HP(p);
-            for (int h = tid; h < HP(p); h += B) {
-                double sum = 0.0;
-                for (int k = 0; k < A; ++k) sum += (double)Sb[(size_t)k * HP(p) + h];
-                const double r = rp[h];
-                for (int k = 0; k < A; ++k) {
-                    const double sg = sum > 0.0 ? (double)Sb[(size_t)k * HP(p) + h] / sum : 1.0 / (double)A;
-                    reach[(size_t)(nd.first + k) * HS + OFF(p) + h] = r * sg;
-                }
-            }
-        } else if (nd.type == MTT_NODE_CHANCE) {
-            for (int k = 0; k < nd.na; ++k) {
-                const int card = nodes[nd.first + k].dealt;
-                for (int p = 0; p < 2; ++p) {
-                    const double* rp = reach + (size_t)(p ? nd.reach_src1 : nd.reach_src0) * HS + OFF(p);
-                    double* ch = reach + (size_t)(nd.first + k) * HS + OFF(p);
-                    for (int h = tid; h < HP(p); h += B) ch[h] = blocked_zero(hc[OFF(p) + h], card, rp[h]);
-                }
-            }
-        }
-    }
-    __syncthreads();
-    for (int n = 0; n < nn; ++n) {
-        const DNode nd = load_node(nodes + n);
-        if (nd.type != MTT_NODE_FOLD && nd.type != MTT_NODE_SHOWDOWN) continue;
-        const int v = tab_variant(sd.river, nd.dealt);
-        const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)v * sd.tab_vsize, sd.H0, sd.H1);
-        eval_terminal<double>(sd, nd, n, tv, reach, br, ev, HS, MTT_SEM_CORRECT, sm_r, sm_x, wbuf, tid, B);
-    }
-    for (int n = nn - 1; n >= 0; --n) {
-        const DNode nd = load_node(nodes + n);
-        if (nd.type == MTT_NODE_DECISION) {
-            const int p = nd.player, o = 1 - p, A = nd.na;
-            const float* Sb = SP(p) + (size_t)nd.row * HP(p);
-            for (int h = tid; h < HP(p); h += B) {
-                double sum = 0.0;
-                for (int k = 0; k < A; ++k) sum += (double)Sb[(size_t)k * HP(p) + h];
-                double best = -1e300, e = 0.0;
-                for (int k = 0; k < A; ++k) {
-                    const size_t c = (size_t)(nd.first + k) * HS + OFF(p) + h;
-                    const double sg = sum > 0.0 ? (double)Sb[(size_t)k * HP(p) + h] / sum : 1.0 / (double)A;
-                    best = fmax(best, br[c]);
-                    e += sg * ev[c];
-                }
-                br[(size_t)n * HS + OFF(p) + h] = best;
-                ev[(size_t)n * HS + OFF(p) + h] = e;
-            }
-            for (int h = tid; h < HP(o); h += B) {
-                double sb = 0.0, se = 0.0;
-                for (int k = 0; k < A; ++k) {
-                    const size_t c = (size_t)(nd.first + k) * HS + OFF(o) + h;
-                    sb += br[c];
-                    se += ev[c];
-                }
-                br[(size_t)n * HS + OFF(o) + h] = sb;
-                ev[(size_t)n * HS + OFF(o) + h] = se;
-            }
-        } else if (nd.type == MTT_NODE_CHANCE) {
-            for (int p = 0; p < 2; ++p)
-                for (int h = tid; h < HP(p); h += B) {
-                    const uint64_t m = hand_mask(hc[OFF(p) + h]);
-                    double sb = 0.0, se = 0.0;
-                    for (int k = 0; k < nd.na; ++k) {
-                        const int card = nodes[nd.first + k].dealt;
-                        if ((m >> card) & 1ull) continue;
-                        const size_t c = (size_t)(nd.first + k) * HS + OFF(p) + h;
-                        sb += br[c];
-                        se += ev[c];
-                    }
-                    br[(size_t)n * HS + OFF(p) + h] = sb / div;
-                    ev[(size_t)n * HS + OFF(p) + h] = se / div;
-                }
-        }
-    }
-    // compatible range mass: a fold-like terminal with payoff 1 for P0 at the root
-    {
-        DNode z{};
-        z.type = MTT_NODE_FOLD;
-        z.wmask = 1;
-        z.pot = 1.0f;
-        z.reach_src0 = 0;
-        z.reach_src1 = 0;
-        z.dealt = -1;
-        const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)tab_variant(sd.river, -1) * sd.tab_vsize,
-                                    sd.H0, sd.H1);
-        eval_terminal<double>(sd, z, nn, tv, reach, br, nullptr, HS, MTT_SEM_CORRECT, sm_r, sm_x, wbuf, tid, B);
-    }
+    // Z: P0's hands against P1's range, a fold terminal with payoff 1
+    DNode z{};
+    z.type = MTT_NODE_FOLD;
+    z.wmask = 1;
+    z.pot = 1.0f;
+    z.dealt = -1;
+    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)tab_variant(sd.river, -1) * sd.tab_vsize, sd.H0, sd.H1);
+    double* X = reinterpret_cast<double*>(smem);
+    double* zm = br + (size_t)nn * HS;
+    cta_terminal<double, double, double>(term_info(sd, z), tv, 0, reach + OFF(1), zm, nullptr, X, wb,
+                                         MTT_SEM_CORRECT, tid);
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int h = tid; h < sd.H0; h += B) {
+    for (int h = tid; h < sd.H0; h += TT) {
         const double r = reach[h];
         acc[0] += r * br[h];
         acc[2] += r * ev[h];
-        acc[4] += r * br[(size_t)nn * HS + h];
+        acc[4] += r * zm[h];
     }
-    for (int h = tid; h < sd.H1; h += B) {
-        const double r = reach[sd.Hp0 + h];
-        acc[1] += r * br[sd.Hp0 + h];
-        acc[3] += r * ev[sd.Hp0 + h];
+    for (int h = tid; h < sd.H1; h += TT) {
+        const double r = reach[OFF(1) + h];
+        acc[1] += r * br[OFF(1) + h];
+        acc[3] += r * ev[OFF(1) + h];
     }
-    double tot[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) tot[k] = block_sum<double>(acc[k], wbuf, tid, B);
+    for (int k = 0; k < 5; ++k) acc[k] = cta_sum(acc[k], wb, tid);
     if (tid == 0) {
-        const double Z = tot[4] > 0.0 ? tot[4] : 1.0;
+        const double Z = acc[4] > 0.0 ? acc[4] : 1.0;
         double* o = a.results + (size_t)s * 6;
-        o[0] = tot[0] / Z;
-        o[1] = tot[1] / Z;
-        o[2] = tot[2] / Z;
-        o[3] = tot[3] / Z;
-        o[4] = tot[4];
+        o[0] = acc[0] / Z;
+        o[1] = acc[1] / Z;
+        o[2] = acc[2] / Z;
+        o[3] = acc[3] / Z;
+        o[4] = acc[4];
         o[5] = 0.5 * (o[0] + o[1]) / (double)sd.pot;
     }
-    __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_batch_br(BatchDev a) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    __shared__ int s_item;
-    const int tid = threadIdx.x, B = blockDim.x;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.queue + 1, 1);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= a.n_sub) return;
-        const int s = a.order ? a.order[item] : item;
-        const SubDesc sd = a.desc[s];
-        br_one(a, sd, s, smem, tid, B);
-    }
-}
+#undef HP
+#undef HH
+#undef OFF
+#undef SRC
 
-// ====================================================================== host
-struct SubPack {
-    std::vector<DNode> nodes;
-    std::vector<uint8_t> tab;
-    std::vector<uint16_t> hcards;
-    std::vector<float> range;
-    SubDesc d{};
-    int status = MTT_OK;
+#include "solver_pack.cuh"
+
+template <typename T>
+struct LevelLists {                  // work lists per depth, concatenated on the device
+    T* d = nullptr;
+    long long cap = 0;               // allocated entries
+    std::vector<long long> off;      // size levels + 1
 };
 
-static int pad4(int h) { return (h + 3) & ~3; }
+// Host copies of every work list, built once per batch.  The continuation
+// rounds of a gate-enforced solve upload the part that belongs to the
+// subgames still above the exploitability target.
+struct HostLists {
+    std::vector<std::vector<FwdItem>> fi, fsim, fal[2];
+    std::vector<std::vector<BwdItem>> bsim, bal[2];
+    std::vector<std::vector<Task>> bf, bb;
+    std::vector<TermItem> titems;    // ascending hand count
+    std::vector<int2> terms;
+};
 
-static void build_variant(const uint8_t* board, int nboard, int dealt, const int H[2],
-                          const std::vector<uint16_t> cards[2], const std::vector<uint16_t> combos[2], uint8_t* out) {
-    std::vector<uint32_t> sc[2];
-    for (int p = 0; p < 2; ++p) {
-        sc[p].resize(H[p]);
-        for (int h = 0; h < H[p]; ++h) {
-            const int c1 = cards[p][h] & 0xFF, c2 = cards[p][h] >> 8;
-            if (dealt >= 0 && (c1 == dealt || c2 == dealt)) { sc[p][h] = 0u; continue; }
-            Planes pl; planes_clear(pl);
-            for (int k = 0; k < nboard; ++k) planes_add(pl, board[k]);
-            if (dealt >= 0) planes_add(pl, dealt);
-            planes_add(pl, c1);
-            planes_add(pl, c2);
-            sc[p][h] = score_planes(pl);
-        }
-    }
-    TabView tv = tab_view(out, H[0], H[1]);
-    std::vector<uint16_t> sorted[2], cl[2], seg[2];
-    std::vector<uint32_t> ssc[2], clsc[2];
-    for (int p = 0; p < 2; ++p) {
-        sorted[p].resize(H[p]);
-        std::iota(sorted[p].begin(), sorted[p].end(), (uint16_t)0);
-        std::stable_sort(sorted[p].begin(), sorted[p].end(), [&](uint16_t x, uint16_t y) { return sc[p][x] < sc[p][y]; });
-        ssc[p].resize(H[p]);
-        for (int i = 0; i < H[p]; ++i) ssc[p][i] = sc[p][sorted[p][i]];
-        // per card lists in rank order
-        std::vector<std::vector<uint16_t>> by(52);
-        for (int i = 0; i < H[p]; ++i) {
-            const uint16_t h = sorted[p][i];
-            by[cards[p][h] & 0xFF].push_back(h);
-            by[cards[p][h] >> 8].push_back(h);
-        }
-        seg[p].assign(54, 0);
-        cl[p].clear();
-        for (int c = 0; c < 52; ++c) {
-            seg[p][c] = (uint16_t)cl[p].size();
-            for (uint16_t h : by[c]) cl[p].push_back(h);
-        }
-        seg[p][52] = seg[p][53] = (uint16_t)cl[p].size();
-        clsc[p].resize(cl[p].size());
-        for (size_t e = 0; e < cl[p].size(); ++e) clsc[p][e] = sc[p][cl[p][e]];
-        std::memcpy(const_cast<uint16_t*>(tv.sorted[p]), sorted[p].data(), 2 * (size_t)H[p]);
-        std::memcpy(const_cast<uint16_t*>(tv.cl[p]), cl[p].data(), 2 * cl[p].size());
-        std::memcpy(const_cast<uint16_t*>(tv.seg[p]), seg[p].data(), 2 * 54);
-    }
-    for (int q = 0; q < 2; ++q) {
-        const int o = 1 - q;
-        Entry* ent = const_cast<Entry*>(tv.ent[q]);
-        for (int h = 0; h < H[q]; ++h) {
-            Entry e{};
-            const int c1 = cards[q][h] & 0xFF, c2 = cards[q][h] >> 8;
-            e.c1 = (uint8_t)c1;
-            e.c2 = (uint8_t)c2;
-            if (dealt >= 0 && (c1 == dealt || c2 == dealt)) {
-                e.lt = e.le = 0xFFFFu;
-                e.same = -1;
-                ent[h] = e;
-                continue;
-            }
-            const uint32_t s = sc[q][h];
-            e.lt = (uint16_t)(std::lower_bound(ssc[o].begin(), ssc[o].end(), s) - ssc[o].begin());
-            e.le = (uint16_t)(std::upper_bound(ssc[o].begin(), ssc[o].end(), s) - ssc[o].begin());
-            auto seg_pos = [&](int c, bool upper) {
-                auto b = clsc[o].begin() + seg[o][c], en = clsc[o].begin() + seg[o][c + 1];
-                return (uint8_t)((upper ? std::upper_bound(b, en, s) : std::lower_bound(b, en, s)) - b);
-            };
-            e.ltc1 = seg_pos(c1, false);
-            e.lec1 = seg_pos(c1, true);
-            e.ltc2 = seg_pos(c2, false);
-            e.lec2 = seg_pos(c2, true);
-            const uint16_t cid = combos[q][h];
-            auto it = std::lower_bound(combos[o].begin(), combos[o].end(), cid);
-            e.same = (it != combos[o].end() && *it == cid) ? (int16_t)(it - combos[o].begin()) : (int16_t)-1;
-            ent[h] = e;
-        }
-    }
-}
-
-static void combo_cards(int id, int& c1, int& c2) {
-    int a = 0, row = 51, k = id;
-    while (k >= row) { k -= row; ++a; --row; }
-    c1 = a;
-    c2 = a + 1 + k;
-}
-
-static void pack_one(const mtt_subgame& g, SubPack& sp) {
-    sp.status = MTT_OK;
-    int rows[2] = {g.rows[0], g.rows[1]};
-    if (!g.nodes || g.n_nodes <= 0 || (g.nboard != 5 && g.nboard != 4)) { sp.status = MTT_ERR_INVALID; return; }
-    int st = validate_tree(g.nodes, g.n_nodes, rows);
-    if (st) { sp.status = st; return; }
-    uint64_t bm = 0;
-    for (int k = 0; k < g.nboard; ++k) {
-        if (g.board[k] > 51 || ((bm >> g.board[k]) & 1ull)) { sp.status = MTT_ERR_INVALID; return; }
-        bm |= 1ull << g.board[k];
-    }
-    const int H[2] = {g.H[0], g.H[1]};
-    std::vector<uint16_t> combos[2], cards[2];
-    for (int p = 0; p < 2; ++p) {
-        if (H[p] < 1 || H[p] > 1326 || !g.combos[p] || !g.ranges[p]) { sp.status = MTT_ERR_INVALID; return; }
-        combos[p].assign(g.combos[p], g.combos[p] + H[p]);
-        cards[p].resize(H[p]);
-        for (int h = 0; h < H[p]; ++h) {
-            const int id = combos[p][h];
-            if (id >= 1326 || (h > 0 && combos[p][h - 1] >= id)) { sp.status = MTT_ERR_INVALID; return; }
-            int c1, c2;
-            combo_cards(id, c1, c2);
-            if (((bm >> c1) & 1ull) || ((bm >> c2) & 1ull)) { sp.status = MTT_ERR_INVALID; return; }
-            const float r = g.ranges[p][h];
-            if (!(r >= 0.0f) || !std::isfinite(r)) { sp.status = MTT_ERR_INVALID; return; }
-            cards[p][h] = (uint16_t)(c1 | (c2 << 8));
-        }
-    }
-    const int nn = g.n_nodes;
-    const int Hp[2] = {pad4(H[0]), pad4(H[1])};
-    // nodes
-    sp.nodes.assign(nn, DNode{});
-    std::vector<int> rsrc0(nn, 0), rsrc1(nn, 0), dealt(nn, -1);
-    for (int i = 0; i < nn; ++i) {
-        const mtt_node& m = g.nodes[i];
-        DNode& d = sp.nodes[i];
-        d.type = m.type;
-        d.player = m.player;
-        d.na = (m.type == MTT_NODE_DECISION || m.type == MTT_NODE_CHANCE) ? m.num_actions : 0;
-        d.wmask = m.active_mask;
-        d.first = m.children_offset;
-        d.row = m.infoset_offset;
-        d.pot = m.pot_size;
-        d.c0 = m.committed[0];
-        d.c1 = m.committed[1];
-        if (m.type == MTT_NODE_DECISION && m.num_actions > MAXA) { sp.status = MTT_ERR_UNSUPPORTED; return; }
-        if (m.type == MTT_NODE_CHANCE && g.nboard != 4) { sp.status = MTT_ERR_INVALID; return; }
-    }
-    for (int i = 0; i < nn; ++i) {
-        const mtt_node& m = g.nodes[i];
-        if (m.type == MTT_NODE_DECISION) {
-            for (int k = 0; k < m.num_actions; ++k) {
-                const int c = m.children_offset + k;
-                rsrc0[c] = m.player == 0 ? c : rsrc0[i];
-                rsrc1[c] = m.player == 1 ? c : rsrc1[i];
-                dealt[c] = dealt[i];
-            }
-        } else if (m.type == MTT_NODE_CHANCE) {
-            for (int k = 0; k < m.num_actions; ++k) {
-                const int c = m.children_offset + k;
-                rsrc0[c] = c;
-                rsrc1[c] = c;
-                dealt[c] = g.nodes[c].turn_idx;
-                if (dealt[c] < 0 || dealt[c] > 51 || ((bm >> dealt[c]) & 1ull)) { sp.status = MTT_ERR_INVALID; return; }
-            }
-        }
-    }
-    for (int i = 0; i < nn; ++i) {
-        sp.nodes[i].reach_src0 = rsrc0[i];
-        sp.nodes[i].reach_src1 = rsrc1[i];
-        sp.nodes[i].dealt = (int16_t)dealt[i];
-        // a turn subgame cannot reach a showdown before the river is dealt
-        if (g.nboard == 4 && g.nodes[i].type == MTT_NODE_SHOWDOWN && dealt[i] < 0) { sp.status = MTT_ERR_INVALID; return; }
-    }
-    // tables
-    const int vsize = tab_variant_bytes(H[0], H[1]);
-    const int nvar = g.nboard == 5 ? 1 : 53;
-    sp.tab.assign((size_t)vsize * nvar, 0);
-    if (g.nboard == 5) {
-        build_variant(g.board, 5, -1, H, cards, combos, sp.tab.data());
-    } else {
-        for (int c = 0; c < 52; ++c) {
-            if ((bm >> c) & 1ull) continue;
-            build_variant(g.board, 4, c, H, cards, combos, sp.tab.data() + (size_t)vsize * c);
-        }
-        build_variant(g.board, 4, -1, H, cards, combos, sp.tab.data() + (size_t)vsize * 52);
-    }
-    sp.hcards.assign((size_t)Hp[0] + Hp[1], 0xFFFFu);
-    sp.range.assign((size_t)Hp[0] + Hp[1], 0.0f);
-    for (int h = 0; h < H[0]; ++h) { sp.hcards[h] = cards[0][h]; sp.range[h] = g.ranges[0][h]; }
-    for (int h = 0; h < H[1]; ++h) { sp.hcards[Hp[0] + h] = cards[1][h]; sp.range[Hp[0] + h] = g.ranges[1][h]; }
-    SubDesc& d = sp.d;
-    d.n_nodes = nn;
-    d.H0 = H[0]; d.H1 = H[1];
-    d.Hp0 = Hp[0]; d.Hp1 = Hp[1];
-    d.rows0 = rows[0]; d.rows1 = rows[1];
-    d.tab_vsize = vsize;
-    d.n_live = 52 - g.nboard;
-    d.river = g.nboard == 5 ? 1 : 0;
-    d.pot = g.nodes[0].pot_size;
-}
+struct ListSet {
+    LevelLists<FwdItem> f_init, f_sim, f_alt[2];
+    LevelLists<BwdItem> b_sim, b_alt[2];
+    LevelLists<Task> br_fwd, br_bwd;
+    TermItem* titems = nullptr;
+    long long titems_cap = 0;
+    int2* terms = nullptr;
+    long long terms_cap = 0;
+    int n_terms = 0;
+    std::vector<int> tb_start, tb_count, tb_smem;   // terminal buckets: offset, size, shared bytes
+    int* subs = nullptr;
+    long long subs_cap = 0;
+    int n_subs = 0;
+};
 
 }  // namespace mtt
 
 using namespace mtt;
 
+// ====================================================================== host driver
 struct mtt_batch {
     int n = 0;
-    int device = 0;
     SubDesc* d_desc = nullptr;
-    int* d_order = nullptr;
     DNode* d_nodes = nullptr;
     uint8_t* d_tabs = nullptr;
     uint16_t* d_hcards = nullptr;
@@ -802,19 +791,21 @@ struct mtt_batch {
     float* d_S = nullptr;
     double* d_darena = nullptr;
     double* d_results = nullptr;
-    int* d_queue = nullptr;
-    float* d_iter = nullptr;        // iteration weights of direct solves
+    int* d_iter = nullptr;
+    int* d_err = nullptr;             // bounded-wait error word of the staged kernels
+    float* d_iter_tab = nullptr;
     int iter_cap = 0;
-    float* d_iter_graph = nullptr;  // owned by the captured graph
+    int levels = 0;
+    HostLists host;
+    ListSet full, act;
     std::vector<SubDesc> desc;
-    int max_hsum = 0;
-    long long device_bytes = 0;
-    long long iter_bytes = 0;
+    std::vector<int> iters_done;
+    int max_h = 0;
+    long long device_bytes = 0, iter_bytes = 0;
     int tuned_threads = 0;
-    // graph cache
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec = nullptr;   // one iteration over the full lists
     mtt_solve_params gparams{};
-    cudaStream_t gstream = nullptr;
+    int gthreads = 0;
 };
 
 namespace mtt {
@@ -826,84 +817,311 @@ static int dalloc(T** p, size_t count, long long& total) {
     return MTT_OK;
 }
 
+static void free_set(ListSet& L) {
+    cudaFree(L.f_init.d); cudaFree(L.f_sim.d); cudaFree(L.b_sim.d);
+    for (int u = 0; u < 2; ++u) { cudaFree(L.f_alt[u].d); cudaFree(L.b_alt[u].d); }
+    cudaFree(L.br_fwd.d); cudaFree(L.br_bwd.d); cudaFree(L.titems); cudaFree(L.terms); cudaFree(L.subs);
+}
+
 static void free_batch(mtt_batch* b) {
     if (!b) return;
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    cudaFree(b->d_desc); cudaFree(b->d_order); cudaFree(b->d_nodes); cudaFree(b->d_tabs);
-    cudaFree(b->d_hcards); cudaFree(b->d_ranges); cudaFree(b->d_arena); cudaFree(b->d_R);
-    cudaFree(b->d_S); cudaFree(b->d_darena); cudaFree(b->d_results); cudaFree(b->d_queue);
-    cudaFree(b->d_iter);
-    cudaFree(b->d_iter_graph);
+    cudaFree(b->d_desc); cudaFree(b->d_nodes); cudaFree(b->d_tabs); cudaFree(b->d_hcards);
+    cudaFree(b->d_ranges); cudaFree(b->d_arena); cudaFree(b->d_R); cudaFree(b->d_S);
+    cudaFree(b->d_darena); cudaFree(b->d_results); cudaFree(b->d_iter); cudaFree(b->d_iter_tab);
+    cudaFree(b->d_err);
+    free_set(b->full);
+    free_set(b->act);
     delete b;
 }
 
-// Per-iteration scalars (t, DCFR positive/negative regret discounts and the
-// strategy-sum discount), computed on the host in double exactly as the oracle does.
-static int fill_iter_table(float** dst, int* cap, const mtt_solve_params& p, cudaStream_t st) {
-    if (p.iters > *cap || !*dst) {
-        if (*dst) { MTT_TRY_CUDA(cudaStreamSynchronize(st)); cudaFree(*dst); *dst = nullptr; }
-        MTT_TRY_CUDA(cudaMalloc(dst, sizeof(float) * 4 * (size_t)std::max(p.iters, 1)));
-        *cap = std::max(p.iters, 1);
+template <typename T>
+static int grow(T** d, long long* cap, long long need, long long& total) {
+    if (need <= *cap && *d) return MTT_OK;
+    cudaFree(*d);
+    *d = nullptr;
+    *cap = 0;
+    MTT_TRY(dalloc(d, (size_t)std::max(need, 1LL), total));
+    *cap = std::max(need, 1LL);
+    return MTT_OK;
+}
+
+// Upload the per-depth lists, keeping the entries whose subgame is active
+// (all when `active` is null).
+template <typename T, typename SubOf>
+static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv, const std::vector<char>* active,
+                         SubOf sub_of, long long& total) {
+    std::vector<T> flat;
+    L.off.assign(lv.size() + 1, 0);
+    for (size_t d = 0; d < lv.size(); ++d) {
+        for (const T& x : lv[d])
+            if (!active || (*active)[sub_of(x)]) flat.push_back(x);
+        L.off[d + 1] = (long long)flat.size();
     }
-    std::vector<float> tab(4 * (size_t)std::max(p.iters, 1), 0.0f);
-    for (int t = 1; t <= p.iters; ++t) {
+    MTT_TRY(grow(&L.d, &L.cap, (long long)flat.size(), total));
+    if (!flat.empty()) MTT_TRY_CUDA(cudaMemcpy(L.d, flat.data(), sizeof(T) * flat.size(), cudaMemcpyHostToDevice));
+    return MTT_OK;
+}
+
+static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, long long& total) {
+    const HostLists& H = b->host;
+    auto fsub = [](const FwdItem& x) { return x.sub; };
+    auto bsub = [](const BwdItem& x) { return x.sub; };
+    auto tsub = [](const Task& x) { return x.sub; };
+    MTT_TRY(upload_levels(L.f_init, H.fi, active, fsub, total));
+    MTT_TRY(upload_levels(L.f_sim, H.fsim, active, fsub, total));
+    MTT_TRY(upload_levels(L.b_sim, H.bsim, active, bsub, total));
+    for (int u = 0; u < 2; ++u) {
+        MTT_TRY(upload_levels(L.f_alt[u], H.fal[u], active, fsub, total));
+        MTT_TRY(upload_levels(L.b_alt[u], H.bal[u], active, bsub, total));
+    }
+    MTT_TRY(upload_levels(L.br_fwd, H.bf, active, tsub, total));
+    MTT_TRY(upload_levels(L.br_bwd, H.bb, active, tsub, total));
+    std::vector<TermItem> ti;
+    std::vector<int2> tm;
+    std::vector<int> subs;
+    for (const TermItem& t : H.titems) if (!active || (*active)[t.sub]) ti.push_back(t);
+    for (const int2& t : H.terms) if (!active || (*active)[t.y]) tm.push_back(t);
+    for (int i = 0; i < b->n; ++i) if (!active || (*active)[i]) subs.push_back(i);
+    MTT_TRY(grow(&L.titems, &L.titems_cap, (long long)ti.size(), total));
+    MTT_TRY(grow(&L.terms, &L.terms_cap, (long long)tm.size(), total));
+    MTT_TRY(grow(&L.subs, &L.subs_cap, (long long)subs.size(), total));
+    if (!ti.empty()) MTT_TRY_CUDA(cudaMemcpy(L.titems, ti.data(), sizeof(TermItem) * ti.size(), cudaMemcpyHostToDevice));
+    if (!tm.empty()) MTT_TRY_CUDA(cudaMemcpy(L.terms, tm.data(), sizeof(int2) * tm.size(), cudaMemcpyHostToDevice));
+    if (!subs.empty()) MTT_TRY_CUDA(cudaMemcpy(L.subs, subs.data(), sizeof(int) * subs.size(), cudaMemcpyHostToDevice));
+    L.n_terms = (int)tm.size();
+    L.n_subs = (int)subs.size();
+    // terminal buckets: ascending hand count, three equal-count launches whose
+    // shared memory is sized by their largest terminal
+    L.tb_start.clear(); L.tb_count.clear(); L.tb_smem.clear();
+    const int nt = (int)ti.size(), nb = nt < 3 ? 1 : 3;
+    for (int k = 0; k < nb; ++k) {
+        const int lo = (int)((long long)nt * k / nb), hi = (int)((long long)nt * (k + 1) / nb);
+        int need = 0;
+        for (int i = lo; i < hi; ++i) {
+            const TermItem& t = ti[i];
+            need = std::max(need, term_stage_bytes(t.Hp[1], t.H[1], t.H[0]));
+            need = std::max(need, term_stage_bytes(t.Hp[0], t.H[0], t.H[1]));
+        }
+        L.tb_start.push_back(lo);
+        L.tb_count.push_back(hi - lo);
+        L.tb_smem.push_back(need);
+    }
+    return MTT_OK;
+}
+
+// Per-iteration scalars (strategy-sum weight t^avg_power, DCFR positive and
+// negative regret discounts, DCFR strategy-sum discount), computed on the
+// host in double exactly as the oracle does.
+static int fill_iter_table(mtt_batch* b, const mtt_solve_params& p, int iters, cudaStream_t st) {
+    if (iters > b->iter_cap || !b->d_iter_tab) {
+        if (b->d_iter_tab) { MTT_TRY_CUDA(cudaStreamSynchronize(st)); cudaFree(b->d_iter_tab); b->d_iter_tab = nullptr; }
+        MTT_TRY_CUDA(cudaMalloc(&b->d_iter_tab, sizeof(float) * 4 * (size_t)std::max(iters, 1)));
+        b->iter_cap = std::max(iters, 1);
+        if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }   // captured the old table
+    }
+    std::vector<float> tab(4 * (size_t)std::max(iters, 1), 0.0f);
+    for (int t = 1; t <= iters; ++t) {
         const double tm1 = (double)(t - 1);
         float* e = &tab[4 * (size_t)(t - 1)];
-        e[0] = (float)t;
+        e[0] = (float)std::pow((double)t, (double)p.avg_power);
         e[1] = (float)(std::pow(tm1, (double)p.alpha) / (std::pow(tm1, (double)p.alpha) + 1.0));
         e[2] = (float)(std::pow(tm1, (double)p.beta) / (std::pow(tm1, (double)p.beta) + 1.0));
         e[3] = (float)std::pow(tm1 / (double)t, (double)p.gamma);
     }
-    MTT_TRY_CUDA(cudaMemcpyAsync(*dst, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st));
-    // pageable source: the copy is staged before returning, so `tab` may go
+    // pageable source: the copy is staged before this returns
+    MTT_TRY_CUDA(cudaMemcpyAsync(b->d_iter_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st));
     return MTT_OK;
 }
 
-static size_t solve_smem(const mtt_batch* b) { return sizeof(float) * (size_t)(4 * b->max_hsum + 64); }
-static size_t br_smem(const mtt_batch* b) { return sizeof(double) * (size_t)(4 * b->max_hsum + 64); }
-
-static BatchDev dev_args(const mtt_batch* b, const mtt_solve_params& p, const float* iter_tab) {
-    BatchDev a;
-    a.desc = b->d_desc; a.n_sub = b->n; a.order = b->d_order; a.nodes = b->d_nodes; a.tabs = b->d_tabs;
-    a.hcards = b->d_hcards; a.ranges = b->d_ranges; a.arena = b->d_arena; a.R = b->d_R; a.S = b->d_S;
-    a.darena = b->d_darena; a.results = b->d_results; a.iter_tab = iter_tab; a.iters = p.iters;
-    a.algo = p.algo; a.semantics = p.semantics; a.queue = b->d_queue;
+static SolveDev dev_args(const mtt_batch* b, const mtt_solve_params& p) {
+    SolveDev a;
+    a.desc = b->d_desc; a.nodes = b->d_nodes; a.tabs = b->d_tabs; a.hcards = b->d_hcards; a.ranges = b->d_ranges;
+    a.arena = b->d_arena; a.R = b->d_R; a.S = b->d_S; a.darena = b->d_darena; a.results = b->d_results;
+    a.iter_tab = b->d_iter_tab; a.iter = b->d_iter; a.err = b->d_err; a.algo = p.algo; a.semantics = p.semantics;
     return a;
 }
 
-static int grid_for(const void* kernel, int threads, size_t smem, int n, int* grid) {
-    int dev = 0, sms = 0, per = 0;
-    MTT_TRY_CUDA(cudaGetDevice(&dev));
-    MTT_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MTT_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
-    if (per < 1) return MTT_ERR_UNSUPPORTED;
-    *grid = std::min(n, sms * per);
-    return MTT_OK;
-}
+static int term_xstride(const mtt_batch* b) { return term_scratch(b->max_h); }
 
-static int launch_solve(mtt_batch* b, const mtt_solve_params& p, int threads, cudaStream_t st, const float* iter_tab) {
-    const size_t sm1 = solve_smem(b), sm2 = br_smem(b);
-    if (sm1 > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    if (sm2 > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_batch_br, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-    int g1 = 0, g2 = 0;
-    MTT_TRY(grid_for((const void*)k_batch_solve, threads, sm1, b->n, &g1));
-    const BatchDev a = dev_args(b, p, iter_tab);
-    MTT_TRY_CUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), st));
-    k_batch_solve<<<g1, threads, sm1, st>>>(a);
-    MTT_CHECK_LAUNCH();
-    if (p.exploitability) {
-        MTT_TRY(grid_for((const void*)k_batch_br, threads, sm2, b->n, &g2));
-        k_batch_br<<<g2, threads, sm2, st>>>(a);
+static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelLists<FwdItem>& L, int threads,
+                             cudaStream_t st) {
+    const long long warps = threads / 32;
+    for (int d = 0; d < b->levels; ++d) {
+        const long long n = L.off[d + 1] - L.off[d];
+        if (n == 0) continue;
+        k_fwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
         MTT_CHECK_LAUNCH();
     }
     return MTT_OK;
 }
 
+static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelLists<BwdItem>& L, int threads,
+                             cudaStream_t st) {
+    const long long warps = threads / 32;
+    for (int d = b->levels - 1; d >= 0; --d) {
+        const long long n = L.off[d + 1] - L.off[d];
+        if (n == 0) continue;
+        k_bwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        MTT_CHECK_LAUNCH();
+    }
+    return MTT_OK;
+}
+
+static int launch_term(const ListSet& L, const SolveDev& a, int upd, cudaStream_t st) {
+    for (size_t k = 0; k < L.tb_start.size(); ++k) {
+        if (L.tb_count[k] == 0) continue;
+        k_term<<<L.tb_count[k], TT, L.tb_smem[k], st>>>(a, L.titems + L.tb_start[k], L.tb_count[k], upd);
+        MTT_CHECK_LAUNCH();
+    }
+    return MTT_OK;
+}
+
+// One CFR iteration: per pass forward levels, terminals, backward levels.
+static int launch_iteration(const mtt_batch* b, const ListSet& L, const SolveDev& a, const mtt_solve_params& p,
+                            int threads, cudaStream_t st) {
+    if (p.alternate) {
+        for (int u = 0; u < 2; ++u) {
+            MTT_TRY(launch_levels_fwd(b, a, L.f_alt[u], threads, st));
+            MTT_TRY(launch_term(L, a, 1 << u, st));
+            MTT_TRY(launch_levels_bwd(b, a, L.b_alt[u], threads, st));
+        }
+    } else {
+        MTT_TRY(launch_levels_fwd(b, a, L.f_sim, threads, st));
+        MTT_TRY(launch_term(L, a, 3, st));
+        MTT_TRY(launch_levels_bwd(b, a, L.b_sim, threads, st));
+    }
+    k_next_iter<<<1, 32, 0, st>>>(a);
+    MTT_CHECK_LAUNCH();
+    return MTT_OK;
+}
+
+static int launch_br(const mtt_batch* b, const ListSet& L, const SolveDev& a, int threads, cudaStream_t st) {
+    if (L.n_subs == 0) return MTT_OK;
+    const long long warps = threads / 32;
+    k_br_init<<<L.n_subs, 128, 0, st>>>(a, L.subs, L.n_subs);
+    MTT_CHECK_LAUNCH();
+    for (int d = 0; d < b->levels; ++d) {
+        const long long n = L.br_fwd.off[d + 1] - L.br_fwd.off[d];
+        if (n == 0) continue;
+        k_br_fwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.br_fwd.d + L.br_fwd.off[d], (int)n);
+        MTT_CHECK_LAUNCH();
+    }
+    const size_t smem = sizeof(double) * (size_t)term_xstride(b);
+    if (L.n_terms) {
+        k_br_term<<<L.n_terms, TT, smem, st>>>(a, L.terms, L.n_terms);
+        MTT_CHECK_LAUNCH();
+    }
+    for (int d = b->levels - 1; d >= 0; --d) {
+        const long long n = L.br_bwd.off[d + 1] - L.br_bwd.off[d];
+        if (n == 0) continue;
+        k_br_bwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.br_bwd.d + L.br_bwd.off[d], (int)n);
+        MTT_CHECK_LAUNCH();
+    }
+    k_br_final<<<L.n_subs, TT, smem, st>>>(a, L.subs, L.n_subs);
+    MTT_CHECK_LAUNCH();
+    return MTT_OK;
+}
+
+static int set_smem_attrs(const mtt_batch* b, const ListSet& L) {
+    const size_t t = sizeof(double) * (size_t)term_xstride(b);
+    if (t > 48 * 1024) {
+        MTT_TRY_CUDA(cudaFuncSetAttribute(k_br_term, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t));
+        MTT_TRY_CUDA(cudaFuncSetAttribute(k_br_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t));
+    }
+    int tmax = 0;
+    for (int v : L.tb_smem) tmax = std::max(tmax, v);
+    if (tmax > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_term, cudaFuncAttributeMaxDynamicSharedMemorySize, tmax));
+    return MTT_OK;
+}
+
 static int check_params(const mtt_solve_params* p) {
     if (!p || p->iters < 0 || (p->algo != MTT_ALGO_CFRPLUS && p->algo != MTT_ALGO_DCFR) ||
-        (p->semantics != MTT_SEM_CORRECT && p->semantics != MTT_SEM_REFERENCE))
+        (p->semantics != MTT_SEM_CORRECT && p->semantics != MTT_SEM_REFERENCE) || p->alternate < 0 ||
+        p->alternate > 1 || !(p->avg_power >= 0.0f && p->avg_power <= 8.0f) || !(p->target_expl >= 0.0f) ||
+        p->max_iters < 0 || p->chunk_iters < 0)
         return MTT_ERR_INVALID;
     if (p->threads != 0 && p->threads != 64 && p->threads != 128 && p->threads != 256) return MTT_ERR_INVALID;
+    return MTT_OK;
+}
+
+static int capture_iteration(const mtt_batch* b, const ListSet& L, const SolveDev& a, const mtt_solve_params& p,
+                             int threads, cudaGraphExec_t* out) {
+    cudaStream_t cs;
+    MTT_TRY_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    int s = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    if (!s) s = launch_iteration(b, L, a, p, threads, cs);
+    const int s2 = cuda_status(cudaStreamEndCapture(cs, &g));
+    if (!s) s = s2;
+    if (!s) s = cuda_status(cudaGraphInstantiate(out, g, 0));
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    return s;
+}
+
+static int run_iterations(mtt_batch* b, const ListSet& L, const SolveDev& a, const mtt_solve_params& p, int threads,
+                          int iters, bool graph, bool cached, cudaStream_t st) {
+    if (!graph) {
+        for (int t = 0; t < iters; ++t) MTT_TRY(launch_iteration(b, L, a, p, threads, st));
+        return MTT_OK;
+    }
+    if (cached) {
+        // the graph reads the iteration table, refilled per solve, so only the launch shape matters
+        const bool same = b->gexec && b->gthreads == threads && b->gparams.algo == p.algo &&
+                          b->gparams.semantics == p.semantics && b->gparams.alternate == p.alternate;
+        if (!same) {
+            if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+            MTT_TRY(capture_iteration(b, L, a, p, threads, &b->gexec));
+            b->gparams = p;
+            b->gthreads = threads;
+        }
+        for (int t = 0; t < iters; ++t) MTT_TRY_CUDA(cudaGraphLaunch(b->gexec, st));
+        return MTT_OK;
+    }
+    cudaGraphExec_t ge = nullptr;
+    MTT_TRY(capture_iteration(b, L, a, p, threads, &ge));
+    int s = MTT_OK;
+    for (int t = 0; t < iters && !s; ++t) s = cuda_status(cudaGraphLaunch(ge, st));
+    cudaGraphExecDestroy(ge);
+    return s;
+}
+
+static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, bool graph) {
+    const int threads = p.threads ? p.threads : (b->tuned_threads ? b->tuned_threads : 256);
+    const bool gate = p.exploitability && p.target_expl > 0.0f && p.max_iters > p.iters;
+    const int chunk = p.chunk_iters > 0 ? p.chunk_iters : std::max(p.iters / 2, 1);
+    MTT_TRY(set_smem_attrs(b, b->full));
+    MTT_TRY(fill_iter_table(b, p, gate ? p.max_iters : p.iters, st));
+    const SolveDev a = dev_args(b, p);
+    k_init<<<b->n, 256, 0, st>>>(a, b->n);
+    MTT_CHECK_LAUNCH();
+    MTT_TRY(launch_levels_fwd(b, a, b->full.f_init, threads, st));
+    MTT_TRY(run_iterations(b, b->full, a, p, threads, p.iters, graph, true, st));
+    std::fill(b->iters_done.begin(), b->iters_done.end(), p.iters);
+    if (p.exploitability) MTT_TRY(launch_br(b, b->full, a, threads, st));
+    if (!gate) return MTT_OK;
+    // Gate: subgames still above the target keep iterating, in chunks, on
+    // work lists compacted to them, until they pass or reach max_iters.
+    std::vector<double> res(6 * (size_t)b->n);
+    int done = p.iters;
+    long long scratch = 0;
+    while (done < p.max_iters) {
+        MTT_TRY_CUDA(cudaMemcpyAsync(res.data(), b->d_results, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, st));
+        MTT_TRY_CUDA(cudaStreamSynchronize(st));
+        std::vector<char> active(b->n, 0);
+        int n_act = 0;
+        for (int i = 0; i < b->n; ++i)
+            if (!(res[6 * (size_t)i + 5] <= (double)p.target_expl)) { active[i] = 1; ++n_act; }
+        if (n_act == 0) break;
+        MTT_TRY(build_set(b, b->act, &active, scratch));
+        MTT_TRY(set_smem_attrs(b, b->act));
+        const int it = std::min(chunk, p.max_iters - done);
+        MTT_TRY(run_iterations(b, b->act, a, p, threads, it, graph, false, st));
+        for (int i = 0; i < b->n; ++i) if (active[i]) b->iters_done[i] += it;
+        done += it;
+        MTT_TRY(launch_br(b, b->act, a, threads, st));
+    }
     return MTT_OK;
 }
 }  // namespace mtt
@@ -922,10 +1140,10 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
     for (int i = 0; i < n; ++i) if (packs[i].status) return packs[i].status;
     mtt_batch* b = new mtt_batch();
     b->n = n;
-    cudaGetDevice(&b->device);
-    long long nodes = 0, arena = 0, rs = 0, tabs = 0, hcards = 0, ranges = 0, darena = 0;
+    b->iters_done.assign(n, 0);
+    long long nodes = 0, arena = 0, rs = 0, tabs = 0, hcards = 0, ranges = 0, darena = 0, iter_bytes = 0;
     b->desc.resize(n);
-    long long iter_bytes = 0;
+    int levels = 0;
     for (int i = 0; i < n; ++i) {
         SubDesc d = packs[i].d;
         const long long HS = d.Hp0 + d.Hp1;
@@ -944,19 +1162,128 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
         darena += 3LL * (d.n_nodes + 1) * HS;
         ranges += HS;
         hcards += HS;
-        b->max_hsum = std::max(b->max_hsum, d.H0 + d.H1);
+        b->max_h = std::max(b->max_h, std::max(d.Hp0, d.Hp1));
+        for (int16_t dp : packs[i].depth) levels = std::max(levels, (int)dp + 1);
         b->desc[i] = d;
-        // algorithmic bytes of one iteration (fp32): R,S read+write per
+        // algorithmic bytes of one iteration (fp32): R and S read+write per
         // action-hand of the acting player; per node, reach written+read and
         // CFV written+read for both players
         iter_bytes += 16LL * ((long long)d.rows0 * d.H0 + (long long)d.rows1 * d.H1) +
                       16LL * (long long)d.n_nodes * (d.H0 + d.H1);
     }
     b->iter_bytes = iter_bytes;
+    b->levels = levels;
+    // FP64 best-response warp tasks, solver work items per level, terminal items
+    HostLists& HL = b->host;
+    HL.bf.assign(levels, {}); HL.bb.assign(levels, {});
+    HL.fi.assign(levels, {}); HL.fsim.assign(levels, {}); HL.bsim.assign(levels, {});
+    for (int u = 0; u < 2; ++u) { HL.fal[u].assign(levels, {}); HL.bal[u].assign(levels, {}); }
+    auto addT = [](std::vector<Task>& v, int node, int sub, int groups) {
+        for (int g0 = 0; g0 < groups; g0 += 32) v.push_back(Task{node, sub, g0, 0});
+    };
+    for (int i = 0; i < n; ++i) {
+        const SubDesc& d = b->desc[i];
+        const long long HS = d.Hp0 + d.Hp1, nn = d.n_nodes;
+        const int Hp[2] = {d.Hp0, d.Hp1}, Hh[2] = {d.H0, d.H1}, H4[2] = {d.Hp0 / 4, d.Hp1 / 4};
+        const long long off[2] = {0, d.Hp0}, rsb[2] = {d.rs_base0, d.rs_base1};
+        const long long reach0 = d.arena_base, cfv0 = d.arena_base + nn * HS;
+        const int Hmax = std::max(H4[0], H4[1]);
+        for (int k = 0; k < d.n_nodes; ++k) {
+            const DNode& nd = packs[i].nodes[k];
+            const int gn = (int)d.node_base + k, dp = packs[i].depth[k];
+            const long long src[2] = {nd.reach_src0, nd.reach_src1};
+            if (nd.type == MTT_NODE_DECISION) {
+                const int p = nd.player;
+                FwdItem f{};
+                f.reach_in = reach0 + src[p] * HS + off[p];
+                f.child = reach0 + (long long)nd.first * HS + off[p];
+                f.rows = rsb[p] + (long long)nd.row * Hp[p];
+                f.h4 = H4[p];
+                f.hs4 = (int)(HS / 4);
+                f.na = nd.na;
+                f.sub = i;
+                for (f.g0 = 0; f.g0 < f.h4; f.g0 += 32) {
+                    f.flags = FI_REACH; HL.fi[dp].push_back(f);
+                    f.flags = FI_REACH | FI_SUMS; HL.fsim[dp].push_back(f);
+                    for (int u = 0; u < 2; ++u) { f.flags = (p == u) ? FI_SUMS : FI_REACH; HL.fal[u][dp].push_back(f); }
+                }
+                for (int q = 0; q < 2; ++q) {
+                    BwdItem bw{};
+                    bw.child = cfv0 + (long long)nd.first * HS + off[q];
+                    bw.self = cfv0 + (long long)k * HS + off[q];
+                    bw.rows = q == p ? f.rows : 0;
+                    bw.h4 = H4[q];
+                    bw.hs4 = (int)(HS / 4);
+                    bw.na = nd.na;
+                    bw.flags = q == p ? BI_UPDATE : 0;
+                    bw.sub = i;
+                    for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
+                        HL.bsim[dp].push_back(bw);
+                        HL.bal[q][dp].push_back(bw);
+                    }
+                }
+                addT(HL.bf[dp], gn, i, H4[p]);
+                addT(HL.bb[dp], gn, i, Hmax);
+            } else if (nd.type == MTT_NODE_CHANCE) {
+                for (int p = 0; p < 2; ++p) {
+                    FwdItem f{};
+                    f.reach_in = reach0 + src[p] * HS + off[p];
+                    f.child = reach0 + (long long)nd.first * HS + off[p];
+                    f.hc = d.hcard_base + off[p];
+                    f.h4 = H4[p];
+                    f.hs4 = (int)(HS / 4);
+                    f.na = nd.na;
+                    f.flags = FI_CHANCE;
+                    f.first = (int)d.node_base + nd.first;
+                    f.sub = i;
+                    for (f.g0 = 0; f.g0 < f.h4; f.g0 += 32) {
+                        HL.fi[dp].push_back(f);
+                        HL.fsim[dp].push_back(f);
+                        HL.fal[1 - p][dp].push_back(f);     // pass u recomputes the other player's reach
+                    }
+                    BwdItem bw{};
+                    bw.child = cfv0 + (long long)nd.first * HS + off[p];
+                    bw.self = cfv0 + (long long)k * HS + off[p];
+                    bw.hc = d.hcard_base + off[p];
+                    bw.h4 = H4[p];
+                    bw.hs4 = (int)(HS / 4);
+                    bw.na = nd.na;
+                    bw.flags = BI_CHANCE;
+                    bw.first = (int)d.node_base + nd.first;
+                    bw.div = (float)(d.n_live - 4);
+                    bw.sub = i;
+                    for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
+                        HL.bsim[dp].push_back(bw);
+                        HL.bal[p][dp].push_back(bw);
+                    }
+                }
+                addT(HL.bf[dp], gn, i, Hmax);
+                addT(HL.bb[dp], gn, i, Hmax);
+            } else {
+                HL.terms.push_back(make_int2(gn, i));
+                TermItem t{};
+                for (int p = 0; p < 2; ++p) {
+                    t.ro[p] = reach0 + src[p] * HS + off[p];
+                    t.out[p] = cfv0 + (long long)k * HS + off[p];
+                    t.H[p] = Hh[p];
+                    t.Hp[p] = Hp[p];
+                }
+                t.tab = d.tab_base + (long long)tab_variant(d.river, nd.dealt) * d.tab_vsize;
+                t.pot = nd.pot;
+                t.c0 = nd.c0;
+                t.c1 = nd.c1;
+                t.type_wmask = nd.type | (nd.wmask << 8);
+                t.sub = i;
+                HL.titems.push_back(t);
+            }
+        }
+    }
+    std::stable_sort(HL.titems.begin(), HL.titems.end(), [](const TermItem& x, const TermItem& y) {
+        return std::max(x.Hp[0], x.Hp[1]) < std::max(y.Hp[0], y.Hp[1]);
+    });
     long long total = 0;
     int s = MTT_OK;
     if (!s) s = dalloc(&b->d_desc, n, total);
-    if (!s) s = dalloc(&b->d_order, n, total);
     if (!s) s = dalloc(&b->d_nodes, nodes, total);
     if (!s) s = dalloc(&b->d_tabs, tabs, total);
     if (!s) s = dalloc(&b->d_hcards, hcards, total);
@@ -966,10 +1293,12 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
     if (!s) s = dalloc(&b->d_S, rs, total);
     if (!s) s = dalloc(&b->d_darena, darena, total);
     if (!s) s = dalloc(&b->d_results, 6LL * n, total);
-    if (!s) s = dalloc(&b->d_queue, 2, total);
+    if (!s) s = dalloc(&b->d_iter, 1, total);
+    if (!s) s = dalloc(&b->d_err, 1, total);
+    if (!s) s = cuda_status(cudaMemset(b->d_err, 0, sizeof(int)));
+    if (!s) s = build_set(b, b->full, nullptr, total);
     if (s) { free_batch(b); return s; }
     b->device_bytes = total;
-    // gather host arrays and upload
     {
         std::vector<DNode> hn(nodes);
         std::vector<uint8_t> ht(tabs);
@@ -982,16 +1311,7 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
             std::copy(packs[i].hcards.begin(), packs[i].hcards.end(), hh.begin() + d.hcard_base);
             std::copy(packs[i].range.begin(), packs[i].range.end(), hr.begin() + d.range_base);
         }
-        // largest subgames first (longest-processing-time order for the work queue)
-        std::vector<int> order(n);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            const SubDesc& a = b->desc[x];
-            const SubDesc& c = b->desc[y];
-            return (long long)a.n_nodes * (a.Hp0 + a.Hp1) > (long long)c.n_nodes * (c.Hp0 + c.Hp1);
-        });
         s = cuda_status(cudaMemcpy(b->d_desc, b->desc.data(), sizeof(SubDesc) * n, cudaMemcpyHostToDevice));
-        if (!s) s = cuda_status(cudaMemcpy(b->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
         if (!s) s = cuda_status(cudaMemcpy(b->d_nodes, hn.data(), sizeof(DNode) * hn.size(), cudaMemcpyHostToDevice));
         if (!s) s = cuda_status(cudaMemcpy(b->d_tabs, ht.data(), ht.size(), cudaMemcpyHostToDevice));
         if (!s) s = cuda_status(cudaMemcpy(b->d_hcards, hh.data(), 2 * hh.size(), cudaMemcpyHostToDevice));
@@ -1007,50 +1327,28 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
 extern "C" int mtt_batch_solve(mtt_batch* b, const mtt_solve_params* prm, void* stream) {
     if (!b) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
-    cudaStream_t st = as_stream(stream);
-    const int threads = prm->threads ? prm->threads : (b->tuned_threads ? b->tuned_threads : 128);
-    MTT_TRY(fill_iter_table(&b->d_iter, &b->iter_cap, *prm, st));
-    return launch_solve(b, *prm, threads, st, b->d_iter);
+    return run_solve(b, *prm, as_stream(stream), false);
 }
 
 extern "C" int mtt_batch_solve_graph(mtt_batch* b, const mtt_solve_params* prm, void* stream) {
     if (!b) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
-    cudaStream_t st = as_stream(stream);
-    const bool same = b->gexec && std::memcmp(&b->gparams, prm, sizeof(*prm)) == 0;
-    if (!same) {
-        if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
-        const int threads = prm->threads ? prm->threads : (b->tuned_threads ? b->tuned_threads : 128);
-        int gcap = 0;
-        if (b->d_iter_graph) { MTT_TRY_CUDA(cudaStreamSynchronize(st)); cudaFree(b->d_iter_graph); b->d_iter_graph = nullptr; }
-        MTT_TRY(fill_iter_table(&b->d_iter_graph, &gcap, *prm, st));
-        MTT_TRY_CUDA(cudaStreamSynchronize(st));
-        // kernel attributes are set outside capture
-        const size_t sm1 = solve_smem(b), sm2 = br_smem(b);
-        if (sm1 > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-        if (sm2 > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_batch_br, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        cudaStream_t cs;
-        MTT_TRY_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        cudaGraph_t graph = nullptr;
-        int s = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        if (!s) s = launch_solve(b, *prm, threads, cs, b->d_iter_graph);
-        const int s2 = cuda_status(cudaStreamEndCapture(cs, &graph));
-        if (!s) s = s2;
-        if (!s) s = cuda_status(cudaGraphInstantiate(&b->gexec, graph, 0));
-        if (graph) cudaGraphDestroy(graph);
-        cudaStreamDestroy(cs);
-        if (s) { b->gexec = nullptr; return s; }
-        b->gparams = *prm;
-    }
-    MTT_TRY_CUDA(cudaGraphLaunch(b->gexec, st));
-    return MTT_OK;
+    return run_solve(b, *prm, as_stream(stream), true);
 }
 
 extern "C" int mtt_batch_results(mtt_batch* b, double* h_out, void* stream) {
     if (!b || !h_out) return MTT_ERR_INVALID;
     cudaStream_t st = as_stream(stream);
+    int err = 0;
     MTT_TRY_CUDA(cudaMemcpyAsync(h_out, b->d_results, sizeof(double) * 6 * (size_t)b->n, cudaMemcpyDeviceToHost, st));
+    MTT_TRY_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     MTT_TRY_CUDA(cudaStreamSynchronize(st));
+    return err ? MTT_ERR_TIMEOUT : MTT_OK;
+}
+
+extern "C" int mtt_batch_iterations(mtt_batch* b, int32_t* h_out) {
+    if (!b || !h_out) return MTT_ERR_INVALID;
+    std::copy(b->iters_done.begin(), b->iters_done.end(), h_out);
     return MTT_OK;
 }
 
@@ -1060,8 +1358,7 @@ extern "C" int mtt_batch_read(mtt_batch* b, int32_t s, float* h_R0, float* h_R1,
     MTT_TRY_CUDA(cudaDeviceSynchronize());
     const SubDesc& d = b->desc[s];
     auto rows_copy = [&](float* dst, const float* src, int rows, int H, int Hp) -> int {
-        if (!dst) return MTT_OK;
-        if (rows == 0) return MTT_OK;
+        if (!dst || rows == 0) return MTT_OK;
         MTT_TRY_CUDA(cudaMemcpy2D(dst, sizeof(float) * H, src, sizeof(float) * Hp, sizeof(float) * H, rows,
                                   cudaMemcpyDeviceToHost));
         return MTT_OK;
@@ -1073,6 +1370,28 @@ extern "C" int mtt_batch_read(mtt_batch* b, int32_t s, float* h_R0, float* h_R1,
     const float* cf = b->d_arena + d.arena_base + (size_t)d.n_nodes * (d.Hp0 + d.Hp1);
     if (h_cfv0) MTT_TRY_CUDA(cudaMemcpy(h_cfv0, cf, sizeof(float) * d.H0, cudaMemcpyDeviceToHost));
     if (h_cfv1) MTT_TRY_CUDA(cudaMemcpy(h_cfv1, cf + d.Hp0, sizeof(float) * d.H1, cudaMemcpyDeviceToHost));
+    return MTT_OK;
+}
+
+extern "C" int mtt_batch_read_vectors(mtt_batch* b, int32_t s, float* h_reach, float* h_cfv) {
+    if (!b || s < 0 || s >= b->n) return MTT_ERR_INVALID;
+    MTT_TRY_CUDA(cudaDeviceSynchronize());
+    const SubDesc& d = b->desc[s];
+    const size_t HS = (size_t)d.Hp0 + d.Hp1, nn = (size_t)d.n_nodes;
+    std::vector<float> arena(2 * nn * HS);
+    MTT_TRY_CUDA(cudaMemcpy(arena.data(), b->d_arena + d.arena_base, sizeof(float) * arena.size(), cudaMemcpyDeviceToHost));
+    std::vector<DNode> nodes(nn);
+    MTT_TRY_CUDA(cudaMemcpy(nodes.data(), b->d_nodes + d.node_base, sizeof(DNode) * nn, cudaMemcpyDeviceToHost));
+    const size_t W = (size_t)d.H0 + d.H1;
+    for (size_t k = 0; k < nn; ++k) {
+        for (int p = 0; p < 2; ++p) {
+            const int H = p ? d.H1 : d.H0;
+            const size_t off = p ? (size_t)d.Hp0 : 0, dst = k * W + (p ? (size_t)d.H0 : 0);
+            const size_t src = (size_t)(p ? nodes[k].reach_src1 : nodes[k].reach_src0);
+            if (h_reach) std::memcpy(h_reach + dst, arena.data() + src * HS + off, sizeof(float) * H);
+            if (h_cfv) std::memcpy(h_cfv + dst, arena.data() + nn * HS + k * HS + off, sizeof(float) * H);
+        }
+    }
     return MTT_OK;
 }
 
@@ -1088,20 +1407,21 @@ extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, voi
     MTT_TRY(check_params(prm));
     cudaStream_t st = as_stream(stream);
     mtt_solve_params p = *prm;
-    p.iters = std::min(std::max(prm->iters, 1), 16);
+    p.iters = std::min(std::max(prm->iters, 1), 8);
     p.exploitability = 0;
-    MTT_TRY(fill_iter_table(&b->d_iter, &b->iter_cap, p, st));
+    p.target_expl = 0.0f;
     const int cands[3] = {64, 128, 256};
     float best_ms = 1e30f;
-    int best = 128;
+    int best = 256;
     cudaEvent_t e0, e1;
     MTT_TRY_CUDA(cudaEventCreate(&e0));
     MTT_TRY_CUDA(cudaEventCreate(&e1));
     int s = MTT_OK;
     for (int c : cands) {
-        if (!s) s = launch_solve(b, p, c, st, b->d_iter);   // warm
+        p.threads = c;
+        if (!s) s = run_solve(b, p, st, false);   // warm
         if (!s) s = cuda_status(cudaEventRecord(e0, st));
-        if (!s) s = launch_solve(b, p, c, st, b->d_iter);
+        if (!s) s = run_solve(b, p, st, false);
         if (!s) s = cuda_status(cudaEventRecord(e1, st));
         if (!s) s = cuda_status(cudaEventSynchronize(e1));
         float ms = 0.f;

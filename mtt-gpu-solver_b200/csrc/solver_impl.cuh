@@ -21,7 +21,7 @@
 
 namespace mtt {
 
-constexpr int MAXA = 8;            // actions per decision node handled by the fused sweeps
+constexpr int MAXA = 16;           // actions per decision node the solver accepts
 
 struct alignas(16) DNode {
     uint8_t type, player, na, wmask;   // wmask: fold winner bit (active_mask)
@@ -53,9 +53,11 @@ struct alignas(16) SubDesc {
     int pad[3];
 };
 
-// Table variant layout (bytes), H0/H1 from the descriptor:
-//   u16 sorted0[H0] | u16 cl0[2*H0] | u16 seg0[54] | u16 sorted1[H1] | u16 cl1[2*H1] | u16 seg1[54]
-//   | Entry e0[H0] (player-0 hands against player-1 lists) | Entry e1[H1]
+// Table variant layout (bytes), H0/H1 from the descriptor; every block starts
+// on a 16-byte boundary so it can be staged with one 1-D bulk copy:
+//   IDX0 = u16 sorted0[H0] | u16 cl0[2*H0] | u16 seg0[54]      (opponent lists of player 0)
+//   IDX1 = the same for player 1
+//   ENT0 = Entry e0[H0] (player-0 hands against player-1 lists), ENT1 = Entry e1[H1]
 struct Entry {
     uint8_t c1, c2, ltc1, lec1, ltc2, lec2;
     uint16_t lt, le;     // lt == 0xFFFF: hand blocked by the dealt card
@@ -70,27 +72,32 @@ struct TabView {
     const Entry* ent[2];
 };
 
+__host__ __device__ inline int round16(int b) { return (b + 15) & ~15; }
+__host__ __device__ inline int tab_idx_bytes(int H) { return round16(2 * (3 * H + 54)); }
+__host__ __device__ inline int tab_ent_bytes(int H) { return round16(12 * H); }
+__host__ __device__ inline int tab_idx_off(int p, int H0) { return p ? tab_idx_bytes(H0) : 0; }
+__host__ __device__ inline int tab_ent_off(int p, int H0, int H1) {
+    return tab_idx_bytes(H0) + tab_idx_bytes(H1) + (p ? tab_ent_bytes(H0) : 0);
+}
 __host__ __device__ inline int tab_variant_bytes(int H0, int H1) {
-    int u16s = (H0 + 2 * H0 + 54) + (H1 + 2 * H1 + 54);
-    int bytes = u16s * 2;
-    bytes = (bytes + 15) & ~15;
-    bytes += 12 * (H0 + H1);
-    return (bytes + 15) & ~15;
+    return tab_idx_bytes(H0) + tab_idx_bytes(H1) + tab_ent_bytes(H0) + tab_ent_bytes(H1);
+}
+
+// Views into one player's index block and entry block (global or shared memory).
+__host__ __device__ inline void tab_idx_view(const uint8_t* blk, int H, const uint16_t** sorted,
+                                             const uint16_t** cl, const uint16_t** seg) {
+    const uint16_t* u = reinterpret_cast<const uint16_t*>(blk);
+    *sorted = u;
+    *cl = u + H;
+    *seg = u + 3 * H;
 }
 
 __host__ __device__ inline TabView tab_view(const uint8_t* base, int H0, int H1) {
     TabView v;
-    const uint16_t* u = reinterpret_cast<const uint16_t*>(base);
-    v.sorted[0] = u; u += H0;
-    v.cl[0] = u; u += 2 * H0;
-    v.seg[0] = u; u += 54;
-    v.sorted[1] = u; u += H1;
-    v.cl[1] = u; u += 2 * H1;
-    v.seg[1] = u; u += 54;
-    size_t off = (size_t)((const uint8_t*)u - base);
-    off = (off + 15) & ~(size_t)15;
-    v.ent[0] = reinterpret_cast<const Entry*>(base + off);
-    v.ent[1] = v.ent[0] + H0;
+    tab_idx_view(base + tab_idx_off(0, H0), H0, &v.sorted[0], &v.cl[0], &v.seg[0]);
+    tab_idx_view(base + tab_idx_off(1, H0), H1, &v.sorted[1], &v.cl[1], &v.seg[1]);
+    v.ent[0] = reinterpret_cast<const Entry*>(base + tab_ent_off(0, H0, H1));
+    v.ent[1] = reinterpret_cast<const Entry*>(base + tab_ent_off(1, H0, H1));
     return v;
 }
 

@@ -342,6 +342,7 @@ static void orc_terminal_values(const orc_ctx* c, int node, int q, const double*
         for (int j = 0; j < Ho; ++j) tot += ro[j];
         for (int h = 0; h < Hq; ++h) {
             double m;
+            if (c->hmask[q][h] & dm) { out[h] = 0.0; continue; }   /* blocked by the dealt card */
             if (sem == ORC_SEM_REFERENCE) m = tot;
             else {
                 m = 0.0;
@@ -405,12 +406,18 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
     double* tv = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
     float chance_div = (prm->semantics == ORC_SEM_REFERENCE) ? (float)(c.n_live - 2) : (float)(c.n_live - 4);
 
+    /* Simultaneous updates (the reference kernels: one forward and one
+     * backward sweep update both players) or alternating updates (CFR+ as
+     * published: P0's pass, then P1's pass against P0's new strategy). */
+    const int n_pass = prm->alternate ? 2 : 1;
     for (int t = 1; t <= prm->iters; ++t) {
-        float w_lin = (float)t;
+        float w_lin = (float)pow((double)t, (double)prm->avg_power);
         double tm1 = (double)(t - 1);
         float dpos = (float)(pow(tm1, (double)prm->alpha) / (pow(tm1, (double)prm->alpha) + 1.0));
         float dneg = (float)(pow(tm1, (double)prm->beta) / (pow(tm1, (double)prm->beta) + 1.0));
         float dstr = (float)pow(tm1 / (double)t, (double)prm->gamma);
+        for (int pass = 0; pass < n_pass; ++pass) {
+        const int upd = prm->alternate ? (1 << pass) : 3;    /* bit p: player p is updated */
         /* forward (parents before children) */
         for (int p = 0; p < 2; ++p) memcpy(reach[p], g->range[p], sizeof(float) * (size_t)H[p]);
         for (int i = 0; i < n; ++i) {
@@ -428,6 +435,7 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
                         float s = (sum > 1e-7f) ? pos[a] / sum : 1.0f / (float)A;   /* :117 */
                         sig[p][(size_t)(row + a) * H[p] + h] = s;
                         reach[p][(size_t)(nd->children_offset + a) * H[p] + h] = rp * s;
+                        if (!((upd >> p) & 1)) continue;
                         float* sp = &S[p][(size_t)(row + a) * H[p] + h];
                         if (prm->algo == ORC_ALGO_DCFR) *sp = fmaf(rp, s, *sp * dstr);
                         else *sp = fmaf(w_lin * rp, s, *sp);                          /* :244 */
@@ -452,6 +460,7 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
             const mtt_node* nd = &g->nodes[i];
             if (nd->type != MTT_NODE_FOLD && nd->type != MTT_NODE_SHOWDOWN) continue;
             for (int q = 0; q < 2; ++q) {
+                if (!((upd >> q) & 1)) continue;
                 int o = 1 - q;
                 for (int j = 0; j < H[o]; ++j) ro[j] = reach[o][(size_t)i * H[o] + j];
                 orc_terminal_values(&c, i, q, ro, prm->semantics, tv);
@@ -463,31 +472,36 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
             const mtt_node* nd = &g->nodes[i];
             if (nd->type == MTT_NODE_DECISION) {                                     /* :220-246 */
                 int p = nd->player, o = 1 - p, A = nd->num_actions, row = nd->infoset_offset;
-                for (int h = 0; h < H[p]; ++h) {
-                    float v = 0.0f;
-                    for (int a = 0; a < A; ++a)
-                        v = fmaf(sig[p][(size_t)(row + a) * H[p] + h],
-                                 cfv[p][(size_t)(nd->children_offset + a) * H[p] + h], v);
-                    cfv[p][(size_t)i * H[p] + h] = v;
-                    for (int a = 0; a < A; ++a) {
-                        float qa = cfv[p][(size_t)(nd->children_offset + a) * H[p] + h];
-                        float* rr = &R[p][(size_t)(row + a) * H[p] + h];
-                        float inst = qa - v;
-                        if (prm->algo == ORC_ALGO_DCFR) {
-                            float disc = *rr * (*rr > 0.0f ? dpos : dneg);
-                            *rr = disc + inst;
-                        } else {
-                            *rr = fmaxf(0.0f, *rr + inst);                          /* :243 */
+                if ((upd >> p) & 1) {
+                    for (int h = 0; h < H[p]; ++h) {
+                        float v = 0.0f;
+                        for (int a = 0; a < A; ++a)
+                            v = fmaf(sig[p][(size_t)(row + a) * H[p] + h],
+                                     cfv[p][(size_t)(nd->children_offset + a) * H[p] + h], v);
+                        cfv[p][(size_t)i * H[p] + h] = v;
+                        for (int a = 0; a < A; ++a) {
+                            float qa = cfv[p][(size_t)(nd->children_offset + a) * H[p] + h];
+                            float* rr = &R[p][(size_t)(row + a) * H[p] + h];
+                            float inst = qa - v;
+                            if (prm->algo == ORC_ALGO_DCFR) {
+                                float disc = *rr * (*rr > 0.0f ? dpos : dneg);
+                                *rr = disc + inst;
+                            } else {
+                                *rr = fmaxf(0.0f, *rr + inst);                      /* :243 */
+                            }
                         }
                     }
                 }
-                for (int h = 0; h < H[o]; ++h) {
-                    float so = 0.0f;
-                    for (int a = 0; a < A; ++a) so += cfv[o][(size_t)(nd->children_offset + a) * H[o] + h];
-                    cfv[o][(size_t)i * H[o] + h] = so;
+                if ((upd >> o) & 1) {
+                    for (int h = 0; h < H[o]; ++h) {
+                        float so = 0.0f;
+                        for (int a = 0; a < A; ++a) so += cfv[o][(size_t)(nd->children_offset + a) * H[o] + h];
+                        cfv[o][(size_t)i * H[o] + h] = so;
+                    }
                 }
             } else if (nd->type == MTT_NODE_CHANCE) {                                /* :205-219 */
-                for (int p = 0; p < 2; ++p)
+                for (int p = 0; p < 2; ++p) {
+                    if (!((upd >> p) & 1)) continue;
                     for (int h = 0; h < H[p]; ++h) {
                         float acc = 0.0f;
                         for (int a = 0; a < nd->num_actions; ++a) {
@@ -497,7 +511,9 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
                         }
                         cfv[p][(size_t)i * H[p] + h] = acc / chance_div;
                     }
+                }
             }
+        }
         }
     }
     if (root_cfv0) memcpy(root_cfv0, cfv[0], sizeof(float) * (size_t)H[0]);

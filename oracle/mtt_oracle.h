@@ -68,6 +68,8 @@ typedef struct orc_cfr_params {
     int32_t algo;
     float   alpha, beta, gamma;
     int32_t semantics;
+    int32_t alternate;    /* 0: simultaneous updates (reference kernels), 1: alternating (CFR+ as published) */
+    float   avg_power;    /* CFR+ strategy-sum weight t^avg_power */
 } orc_cfr_params;
 
 /* Runs iters iterations from zero regrets.  R_p, S_p: [rows_p][H_p].

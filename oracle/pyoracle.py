@@ -30,7 +30,8 @@ class Game(ctypes.Structure):
 
 class CfrParams(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("algo", ctypes.c_int32), ("alpha", ctypes.c_float),
-                ("beta", ctypes.c_float), ("gamma", ctypes.c_float), ("semantics", ctypes.c_int32)]
+                ("beta", ctypes.c_float), ("gamma", ctypes.c_float), ("semantics", ctypes.c_int32),
+                ("alternate", ctypes.c_int32), ("avg_power", ctypes.c_float)]
 
 
 def lib():
@@ -128,9 +129,10 @@ def _combo_cards(ids):
     return _CC[np.asarray(ids, dtype=np.int64)]
 
 
-def cfr_solve(sub, iters, algo=0, alpha=1.5, beta=0.0, gamma=2.0, semantics=0):
+def cfr_solve(sub, iters, algo=0, alpha=1.5, beta=0.0, gamma=2.0, semantics=0, alternate=0, avg_power=1.0):
     gh = _GameHolder(sub)
-    p = CfrParams(int(iters), int(algo), float(alpha), float(beta), float(gamma), int(semantics))
+    p = CfrParams(int(iters), int(algo), float(alpha), float(beta), float(gamma), int(semantics), int(alternate),
+                  float(avg_power))
     R0 = np.zeros((gh.rows[0], gh.H[0]), np.float32); R1 = np.zeros((gh.rows[1], gh.H[1]), np.float32)
     S0 = np.zeros_like(R0); S1 = np.zeros_like(R1)
     c0 = np.zeros(gh.H[0], np.float32); c1 = np.zeros(gh.H[1], np.float32)

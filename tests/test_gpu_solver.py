@@ -1,10 +1,15 @@
 """Batched CFR solver on the GPU vs the CPU oracle.
 
 The oracle restates the reference sweeps (honest_multistreet_solver.cu:88-249)
-with dense O(H^2) showdowns in FP64; the GPU uses rank-order prefix scans
-in FP32.  Tolerances: regrets, strategy sums and counterfactual values agree
-to 1e-4 of the pot (relative 1e-4 on the accumulated sums), the FP64 best
-response agrees to 1e-9 on identical strategy sums.
+with dense O(H^2) showdowns accumulated in FP64; the GPU uses rank-order
+prefix scans in FP32.  Tolerances (all written here):
+  * counterfactual values: 1e-4 of the pot per unit of opponent range mass;
+  * regrets and strategy sums: 1e-4 relative to the largest entry;
+  * the FP64 best response: 1e-9 on identical strategy sums.
+Strict comparisons use few iterations: regret matching's uniform fallback
+(sum of positive regrets <= 1e-7, honest_multistreet_solver.cu:117) and the
+CFR+ clip are discontinuous, so FP32 rounding differences between two valid
+summation orders can later pick different branches for indifferent hands.
 """
 import numpy as np
 import pytest
@@ -24,42 +29,55 @@ def _solve_gpu(mtt, subs, **kw):
     return res, reads
 
 
-def _compare(orc_out, gpu_out, pot, iters):
-    # accumulated quantities grow ~linearly with t (S with t^2 for linear averaging)
-    for key in ("R0", "R1"):
-        a, g = orc_out[key], gpu_out[key]
-        scale = max(1.0, float(np.abs(a).max()))
-        assert np.abs(a - g).max() <= 1e-4 * scale, key
-    for key in ("S0", "S1"):
+def _compare(sub, orc_out, gpu_out):
+    pot = sub["pot"]
+    for key in ("R0", "R1", "S0", "S1"):
         a, g = orc_out[key], gpu_out[key]
         scale = max(1e-12, float(np.abs(a).max()))
         assert np.abs(a - g).max() <= 1e-4 * scale, key
-    for key in ("cfv0", "cfv1"):
-        assert np.abs(orc_out[key] - gpu_out[key]).max() <= TOL_POT * pot, key
+    for q in (0, 1):
+        mass = float(np.sum(sub[f"range{1 - q}"]))
+        d = np.abs(orc_out[f"cfv{q}"] - gpu_out[f"cfv{q}"]).max()
+        assert d <= TOL_POT * pot * mass, (q, d, pot * mass)
 
 
-@pytest.mark.parametrize("iters,algo,sem", [(1, 0, 0), (30, 0, 0), (30, 1, 0), (30, 0, 1), (30, 1, 1)])
-def test_river_small_vs_oracle(mtt, wl, orc, cuda, iters, algo, sem):
+@pytest.mark.parametrize("alternate", [0, 1])
+@pytest.mark.parametrize("algo,sem", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("iters", [1, 4])
+def test_river_vs_oracle(mtt, wl, orc, cuda, iters, algo, sem, alternate):
     sub = wl.river_uniform(seed=3, n_hands=80)
-    res, reads = _solve_gpu(mtt, [sub], iters=iters, algo=algo, semantics=sem, threads=128)
-    o = orc.cfr_solve(sub, iters, algo=algo, semantics=sem)
-    _compare(o, reads[0], sub["pot"], iters)
+    res, reads = _solve_gpu(mtt, [sub], iters=iters, algo=algo, semantics=sem, alternate=alternate, threads=128)
+    o = orc.cfr_solve(sub, iters, algo=algo, semantics=sem, alternate=alternate)
+    _compare(sub, o, reads[0])
     br = orc.best_response(sub, reads[0]["S0"], reads[0]["S1"])
     assert np.allclose(res[0], br, rtol=1e-9, atol=1e-9)
 
 
-def test_uneven_batch_vs_oracle(mtt, wl, orc, cuda):
+@pytest.mark.parametrize("alternate", [0, 1])
+def test_uneven_batch_vs_oracle(mtt, wl, orc, cuda, alternate):
     subs = wl.river_batch(n=6, seed=11, min_support=40, max_support=90, max_sizes=3)
-    res, reads = _solve_gpu(mtt, subs, iters=25, threads=64)
+    res, reads = _solve_gpu(mtt, subs, iters=3, alternate=alternate, threads=64)
     for i, g in enumerate(subs):
-        o = orc.cfr_solve(g, 25)
-        _compare(o, reads[i], g["pot"], 25)
+        o = orc.cfr_solve(g, 3, alternate=alternate)
+        _compare(g, o, reads[i])
         br = orc.best_response(g, reads[i]["S0"], reads[i]["S1"])
         assert np.allclose(res[i], br, rtol=1e-9, atol=1e-9)
 
 
-@pytest.mark.parametrize("threads", [64, 128, 256])
-def test_cta_size_does_not_change_results(mtt, wl, cuda, threads):
+def test_longer_solve_tracks_oracle(mtt, wl, orc, cuda):
+    """After 60 alternating CFR+ iterations both sides agree on exploitability
+    and root EV to 1e-4 of the pot."""
+    subs = wl.river_batch(n=4, seed=17, min_support=60, max_support=120, max_sizes=2)
+    res, reads = _solve_gpu(mtt, subs, iters=60, threads=256)
+    for i, g in enumerate(subs):
+        o = orc.cfr_solve(g, 60, alternate=1)
+        br = orc.best_response(g, o["S0"], o["S1"])
+        assert abs(res[i][5] - br[5]) <= 1e-4, (res[i][5], br[5])
+        assert abs(res[i][2] - br[2]) <= 1e-4 * g["pot"]
+
+
+@pytest.mark.parametrize("threads", [64, 256])
+def test_results_do_not_depend_on_cta_size(mtt, wl, cuda, threads):
     subs = wl.river_batch(n=3, seed=5, min_support=100, max_support=300)
     base_res, base = _solve_gpu(mtt, subs, iters=20, threads=128)
     res, reads = _solve_gpu(mtt, subs, iters=20, threads=threads)
@@ -85,7 +103,8 @@ def test_graph_replay_matches_direct(mtt, wl, cuda):
     assert np.array_equal(s1["S0"], s2["S0"]) and np.array_equal(s1["R1"], s2["R1"])
 
 
-def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda):
+@pytest.mark.parametrize("algo", [0, 1])
+def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda, algo):
     rng = np.random.default_rng(21)
     board = [int(c) for c in rng.choice(52, size=4, replace=False)]
     nodes, rows, _ = mtt.build_tree(60, 100, [0.75], raise_cap=1, street=4, board=board)
@@ -95,12 +114,11 @@ def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda):
     sub = {"nodes": nodes, "rows": rows, "board": board, "combos0": c0, "combos1": c1,
            "range0": rng.dirichlet(np.full(40, 0.3)).astype(np.float32),
            "range1": rng.dirichlet(np.full(36, 0.3)).astype(np.float32), "pot": 60.0}
-    for algo in (0, 1):
-        res, reads = _solve_gpu(mtt, [sub], iters=12, algo=algo, threads=128)
-        o = orc.cfr_solve(sub, 12, algo=algo)
-        _compare(o, reads[0], 60.0, 12)
-        br = orc.best_response(sub, reads[0]["S0"], reads[0]["S1"])
-        assert np.allclose(res[0], br, rtol=1e-8, atol=1e-9)
+    res, reads = _solve_gpu(mtt, [sub], iters=3, algo=algo, threads=128)
+    o = orc.cfr_solve(sub, 3, algo=algo, alternate=1)
+    _compare(sub, o, reads[0])
+    br = orc.best_response(sub, reads[0]["S0"], reads[0]["S1"])
+    assert np.allclose(res[0], br, rtol=1e-8, atol=1e-9)
 
 
 def test_config0_converges_below_0p1_percent(mtt, wl, cuda):
@@ -112,10 +130,34 @@ def test_config0_converges_below_0p1_percent(mtt, wl, cuda):
     assert expl <= 1e-3
 
 
-def test_config2_sample_converges(mtt, wl, cuda):
-    subs = wl.river_batch(n=48, seed=2)
-    res, _ = _solve_gpu(mtt, subs, iters=1000, threads=128)
+def test_config2_sample_reaches_the_gate(mtt, wl, cuda):
+    """1,000 alternating CFR+ iterations, then subgames above 0.1% of the pot
+    continue in 500-iteration chunks until every one passes."""
+    subs = wl.river_batch(n=64, seed=2)
+    b = mtt.RiverBatch(subs)
+    b.solve(mtt.solve_params(iters=1000, threads=256, avg_power=2.0, target_expl=1e-3, max_iters=4000,
+                             chunk_iters=500))
+    res = b.results()
+    its = b.iterations()
+    b.close()
     expl = res[:, 5]
     assert np.isfinite(res).all()
     assert (res[:, 0] >= res[:, 2] - 1e-9).all() and (res[:, 1] >= res[:, 3] - 1e-9).all()
-    assert np.median(expl) <= 1e-3
+    assert (expl <= 1e-3).all(), np.sort(expl)[-5:]
+    assert (its >= 1000).all() and (its[expl > 0] <= 4000).all()
+
+
+def test_continuation_matches_a_longer_solve(mtt, wl, cuda):
+    """A subgame continued by the gate ends exactly where an uninterrupted
+    solve of the same length ends."""
+    subs = wl.river_batch(n=6, seed=4, min_support=80, max_support=200)
+    b = mtt.RiverBatch(subs)
+    b.solve(mtt.solve_params(iters=40, threads=128, target_expl=1e-9, max_iters=60, chunk_iters=20))
+    its = b.iterations()
+    cont = [b.read(i) for i in range(len(subs))]
+    b.close()
+    assert (its == 60).all()
+    res, ref = _solve_gpu(mtt, subs, iters=60, threads=128)
+    for a_, r_ in zip(cont, ref):
+        for k in ("R0", "R1", "S0", "S1"):
+            assert np.array_equal(a_[k], r_[k]), k
