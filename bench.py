@@ -191,11 +191,13 @@ def run_b200(args, rank, world, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    launches0 = batch.launch_count()
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    gpu_launches = batch.launch_count() - launches0
     clocks = clk.stop()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     if pg:
@@ -219,8 +221,9 @@ def run_b200(args, rank, world, local):
     ps = mtt.solve_params(iters=args.iters, threads=threads, exploitability=False, alternate=True, avg_power=2.0)
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
+    batch.solve(ps, graph=True)
     k0.record(stream)
-    batch.solve(ps)
+    batch.solve(ps, graph=True)
     k1.record(stream)
     torch.cuda.synchronize()
     solve_ms = k0.elapsed_time(k1)
@@ -302,7 +305,7 @@ def run_b200(args, rank, world, local):
             "clocks": clocks,
             "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(args.subgames * 6 * 8)},
-            "gpu_launches": 2 * args.steps}
+            "gpu_launches": int(gpu_launches)}
     if rank == 0 and not args.no_cpu_baseline:
         v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, args.cpu_sample or max(os.cpu_count() or 1, 8))
         line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}

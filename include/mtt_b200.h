@@ -235,6 +235,9 @@ int mtt_batch_read_vectors(mtt_batch* b, int32_t s, float* h_reach, float* h_cfv
  * batch (R,S read+write per action-hand; reach and CFV written and read once
  * per player-hand per node). */
 int mtt_batch_info(mtt_batch* b, int64_t* device_bytes, int64_t* iter_bytes);
+/* Kernels launched for this batch since it was created; a graph replay counts
+ * every kernel node it runs. No reference counterpart (instrumentation). */
+int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
 /* Pick the CTA size by timing a few iterations of each candidate on this
  * batch; *threads receives the choice (also used when params.threads == 0). */
 int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads);

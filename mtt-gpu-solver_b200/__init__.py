@@ -255,6 +255,12 @@ class RiverBatch:
         check("mtt_batch_info", lib().mtt_batch_info(self._h, ctypes.byref(db), ctypes.byref(ib)))
         return {"device_bytes": db.value, "iter_bytes": ib.value}
 
+    def launch_count(self):
+        """Kernels launched for this batch so far (graph replays count every node)."""
+        n = ctypes.c_int64()
+        check("mtt_batch_launch_count", lib().mtt_batch_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
     def autotune(self, params, stream=None):
         t = ctypes.c_int32()
         check("mtt_batch_autotune", lib().mtt_batch_autotune(self._h, ctypes.byref(params), _stream(stream),

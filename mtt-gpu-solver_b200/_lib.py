@@ -87,6 +87,7 @@ def lib():
         "mtt_batch_iterations": ([vp, vp], ctypes.c_int),
         "mtt_batch_read_vectors": ([vp, i32, vp, vp], ctypes.c_int),
         "mtt_batch_info": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_launch_count": ([vp, vp], ctypes.c_int),
         "mtt_batch_autotune": ([vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_destroy": ([vp], ctypes.c_int),
     }

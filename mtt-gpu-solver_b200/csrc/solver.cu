@@ -804,8 +804,10 @@ struct mtt_batch {
     long long device_bytes = 0, iter_bytes = 0;
     int tuned_threads = 0;
     cudaGraphExec_t gexec = nullptr;   // one iteration over the full lists
+    int gkernels = 0;                  // kernel nodes in gexec
     mtt_solve_params gparams{};
     int gthreads = 0;
+    mutable long long launches = 0;    // kernels run for this batch (graph replays count every node)
 };
 
 namespace mtt {
@@ -952,6 +954,7 @@ static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelL
         if (n == 0) continue;
         k_fwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     return MTT_OK;
 }
@@ -964,15 +967,17 @@ static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelL
         if (n == 0) continue;
         k_bwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     return MTT_OK;
 }
 
-static int launch_term(const ListSet& L, const SolveDev& a, int upd, cudaStream_t st) {
+static int launch_term(const mtt_batch* b, const ListSet& L, const SolveDev& a, int upd, cudaStream_t st) {
     for (size_t k = 0; k < L.tb_start.size(); ++k) {
         if (L.tb_count[k] == 0) continue;
         k_term<<<L.tb_count[k], TT, L.tb_smem[k], st>>>(a, L.titems + L.tb_start[k], L.tb_count[k], upd);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     return MTT_OK;
 }
@@ -983,16 +988,17 @@ static int launch_iteration(const mtt_batch* b, const ListSet& L, const SolveDev
     if (p.alternate) {
         for (int u = 0; u < 2; ++u) {
             MTT_TRY(launch_levels_fwd(b, a, L.f_alt[u], threads, st));
-            MTT_TRY(launch_term(L, a, 1 << u, st));
+            MTT_TRY(launch_term(b, L, a, 1 << u, st));
             MTT_TRY(launch_levels_bwd(b, a, L.b_alt[u], threads, st));
         }
     } else {
         MTT_TRY(launch_levels_fwd(b, a, L.f_sim, threads, st));
-        MTT_TRY(launch_term(L, a, 3, st));
+        MTT_TRY(launch_term(b, L, a, 3, st));
         MTT_TRY(launch_levels_bwd(b, a, L.b_sim, threads, st));
     }
     k_next_iter<<<1, 32, 0, st>>>(a);
     MTT_CHECK_LAUNCH();
+    ++b->launches;
     return MTT_OK;
 }
 
@@ -1001,25 +1007,30 @@ static int launch_br(const mtt_batch* b, const ListSet& L, const SolveDev& a, in
     const long long warps = threads / 32;
     k_br_init<<<L.n_subs, 128, 0, st>>>(a, L.subs, L.n_subs);
     MTT_CHECK_LAUNCH();
+    ++b->launches;
     for (int d = 0; d < b->levels; ++d) {
         const long long n = L.br_fwd.off[d + 1] - L.br_fwd.off[d];
         if (n == 0) continue;
         k_br_fwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.br_fwd.d + L.br_fwd.off[d], (int)n);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     const size_t smem = sizeof(double) * (size_t)term_xstride(b);
     if (L.n_terms) {
         k_br_term<<<L.n_terms, TT, smem, st>>>(a, L.terms, L.n_terms);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     for (int d = b->levels - 1; d >= 0; --d) {
         const long long n = L.br_bwd.off[d + 1] - L.br_bwd.off[d];
         if (n == 0) continue;
         k_br_bwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.br_bwd.d + L.br_bwd.off[d], (int)n);
         MTT_CHECK_LAUNCH();
+        ++b->launches;
     }
     k_br_final<<<L.n_subs, TT, smem, st>>>(a, L.subs, L.n_subs);
     MTT_CHECK_LAUNCH();
+    ++b->launches;
     return MTT_OK;
 }
 
@@ -1045,8 +1056,11 @@ static int check_params(const mtt_solve_params* p) {
     return MTT_OK;
 }
 
+// Captures one iteration; *kernels = the kernel nodes it holds (captured
+// launches do not run, so they are taken back out of the launch count).
 static int capture_iteration(const mtt_batch* b, const ListSet& L, const SolveDev& a, const mtt_solve_params& p,
-                             int threads, cudaGraphExec_t* out) {
+                             int threads, cudaGraphExec_t* out, int* kernels) {
+    const long long before = b->launches;
     cudaStream_t cs;
     MTT_TRY_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
@@ -1057,6 +1071,8 @@ static int capture_iteration(const mtt_batch* b, const ListSet& L, const SolveDe
     if (!s) s = cuda_status(cudaGraphInstantiate(out, g, 0));
     if (g) cudaGraphDestroy(g);
     cudaStreamDestroy(cs);
+    *kernels = (int)(b->launches - before);
+    b->launches = before;
     return s;
 }
 
@@ -1072,17 +1088,24 @@ static int run_iterations(mtt_batch* b, const ListSet& L, const SolveDev& a, con
                           b->gparams.semantics == p.semantics && b->gparams.alternate == p.alternate;
         if (!same) {
             if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
-            MTT_TRY(capture_iteration(b, L, a, p, threads, &b->gexec));
+            MTT_TRY(capture_iteration(b, L, a, p, threads, &b->gexec, &b->gkernels));
             b->gparams = p;
             b->gthreads = threads;
         }
-        for (int t = 0; t < iters; ++t) MTT_TRY_CUDA(cudaGraphLaunch(b->gexec, st));
+        for (int t = 0; t < iters; ++t) {
+            MTT_TRY_CUDA(cudaGraphLaunch(b->gexec, st));
+            b->launches += b->gkernels;
+        }
         return MTT_OK;
     }
     cudaGraphExec_t ge = nullptr;
-    MTT_TRY(capture_iteration(b, L, a, p, threads, &ge));
+    int kernels = 0;
+    MTT_TRY(capture_iteration(b, L, a, p, threads, &ge, &kernels));
     int s = MTT_OK;
-    for (int t = 0; t < iters && !s; ++t) s = cuda_status(cudaGraphLaunch(ge, st));
+    for (int t = 0; t < iters && !s; ++t) {
+        s = cuda_status(cudaGraphLaunch(ge, st));
+        if (!s) b->launches += kernels;
+    }
     cudaGraphExecDestroy(ge);
     return s;
 }
@@ -1096,6 +1119,7 @@ static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, b
     const SolveDev a = dev_args(b, p);
     k_init<<<b->n, 256, 0, st>>>(a, b->n);
     MTT_CHECK_LAUNCH();
+    ++b->launches;
     MTT_TRY(launch_levels_fwd(b, a, b->full.f_init, threads, st));
     MTT_TRY(run_iterations(b, b->full, a, p, threads, p.iters, graph, true, st));
     std::fill(b->iters_done.begin(), b->iters_done.end(), p.iters);
@@ -1399,6 +1423,12 @@ extern "C" int mtt_batch_info(mtt_batch* b, int64_t* device_bytes, int64_t* iter
     if (!b) return MTT_ERR_INVALID;
     if (device_bytes) *device_bytes = b->device_bytes;
     if (iter_bytes) *iter_bytes = b->iter_bytes;
+    return MTT_OK;
+}
+
+extern "C" int mtt_batch_launch_count(mtt_batch* b, int64_t* launches) {
+    if (!b || !launches) return MTT_ERR_INVALID;
+    *launches = b->launches;
     return MTT_OK;
 }
 
