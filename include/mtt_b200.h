@@ -141,6 +141,23 @@ int mtt_eval7_enumerate(uint64_t* d_hist9, uint64_t* d_checksum, uint32_t* d_key
 int mtt_board_showdown_counts(const uint8_t* d_board, int32_t nboard, const uint8_t* d_hands,
                               int32_t H, int32_t* d_w, int32_t* d_t, int32_t* d_l, void* stream);
 
+/* Same counts as mtt_board_showdown_counts, with no device allocation.  No
+ * counterpart in the reference.  For callers that may not allocate during the
+ * call: a process whose free device memory is already handed to another
+ * pool, or a worker loop that must not stall on, or fail in, the allocator.
+ * The key scratch is a fixed 1 MiB static device array, one per device.
+ * Limit: ceil(C/2) * roundup(H, 64) <= MTT_COUNTS_NOALLOC_MAX_WORDS, where C
+ * is the number of board completions (1 river, 48 turn, 1,176 flop), i.e.
+ * any H <= 1,326 on 4- and 5-card boards and H <= 384 on 3-card boards;
+ * larger sizes return MTT_ERR_UNSUPPORTED before any device work.  The first
+ * call on a device looks up the scratch address with that device current;
+ * make that first call before any stream capture.  Calls that overlap in
+ * time on the same device share the scratch and race: order them on one
+ * stream or serialise them. */
+#define MTT_COUNTS_NOALLOC_MAX_WORDS 262144
+int mtt_board_showdown_counts_noalloc(const uint8_t* d_board, int32_t nboard, const uint8_t* d_hands,
+                                      int32_t H, int32_t* d_w, int32_t* d_t, int32_t* d_l, void* stream);
+
 /* ------------------------------------------------------------ dumper path */
 /* The 1,755 canonical flops with orbit weights, h_out[4*i..] = c1,c2,c3,w
  * (generate_all_1755_flops, src/tools/mtt_ev_dumper.cu:34-51). Host only. */

@@ -76,6 +76,7 @@ def lib():
         "mtt_eval7": ([vp, vp, i64, vp], ctypes.c_int),
         "mtt_eval7_enumerate": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_board_showdown_counts": ([vp, i32, vp, i32, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_board_showdown_counts_noalloc": ([vp, i32, vp, i32, vp, vp, vp, vp], ctypes.c_int),
         "mtt_canonical_flops": ([vp, i32, vp], ctypes.c_int),
         "mtt_flop_ev": ([vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_ev_dump": ([vp, i32, vp, vp], ctypes.c_int),

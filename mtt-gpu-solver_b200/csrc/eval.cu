@@ -15,6 +15,7 @@
 //    accumulation order and host aggregation, reproduced bit-exactly.
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "mtt_bulk.cuh"
@@ -613,6 +614,58 @@ extern "C" int mtt_board_showdown_counts(const uint8_t* d_board, int32_t nboard,
     }
     cudaFreeAsync(keys, st);
     return s;
+}
+
+// ------------------------------------------------ counts without allocation
+// Key scratch of mtt_board_showdown_counts_noalloc: one per device, in the
+// module's static device memory, so a call needs no allocator.  1 MiB.
+static __device__ __align__(256) uint32_t g_counts_scratch[MTT_COUNTS_NOALLOC_MAX_WORDS];
+
+namespace mtt {
+constexpr int kMaxDevices = 64;
+static std::mutex g_counts_scratch_mu;
+static uint32_t* g_counts_scratch_ptr[kMaxDevices] = {};
+
+// Address of this device's scratch, looked up once per device with that device current.
+static int counts_scratch(uint32_t** out) {
+    int dev = 0;
+    MTT_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return MTT_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_counts_scratch_mu);
+    if (!g_counts_scratch_ptr[dev]) {
+        void* p = nullptr;
+        MTT_TRY_CUDA(cudaGetSymbolAddress(&p, g_counts_scratch));
+        g_counts_scratch_ptr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_counts_scratch_ptr[dev];
+    return MTT_OK;
+}
+}  // namespace mtt
+
+extern "C" int mtt_board_showdown_counts_noalloc(const uint8_t* d_board, int32_t nboard, const uint8_t* d_hands,
+                                                 int32_t H, int32_t* d_w, int32_t* d_t, int32_t* d_l,
+                                                 void* stream) {
+    if (nboard < 3 || nboard > 5 || H < 0 || H > 1326) return MTT_ERR_INVALID;
+    if (H == 0) return MTT_OK;
+    if (!d_board || !d_hands || !d_w || !d_t || !d_l) return MTT_ERR_INVALID;
+    const int nrest = 52 - nboard;
+    const int ncomp = nboard == 5 ? 1 : nboard == 4 ? nrest : nrest * (nrest - 1) / 2;
+    const int ncw = (ncomp + 1) / 2;
+    const int Hp = (H + 63) / 64 * 64;
+    if ((long long)ncw * Hp > MTT_COUNTS_NOALLOC_MAX_WORDS) return MTT_ERR_UNSUPPORTED;
+    const int free_cards = nrest - 4;
+    const int n_const = nboard == 5 ? 1 : nboard == 4 ? free_cards : free_cards * (free_cards - 1) / 2;
+    uint32_t* keys = nullptr;
+    MTT_TRY(counts_scratch(&keys));
+    cudaStream_t st = as_stream(stream);
+    // Nothing in the scratch has to start at zero: k_completion_keys writes
+    // all ncw * Hp words before k_board_counts reads any of them.
+    k_completion_keys<<<dim3(Hp / 64, ncw), 64, 0, st>>>(d_board, nboard, d_hands, H, Hp, ncomp, keys);
+    MTT_TRY_CUDA(cudaGetLastError());
+    k_board_counts<<<dim3(Hp / BC_TILE, Hp / BC_TILE), 256, 0, st>>>(keys, ncw, H, Hp, d_hands, d_board, nboard,
+                                                                    n_const, d_w, d_t, d_l);
+    MTT_TRY_CUDA(cudaGetLastError());
+    return MTT_OK;
 }
 
 extern "C" int mtt_canonical_flops(uint8_t* h_out, int32_t capacity, int32_t* n_out) {
