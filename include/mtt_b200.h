@@ -248,10 +248,43 @@ int mtt_batch_read(mtt_batch* b, int32_t s, float* h_R0, float* h_R1, float* h_S
  * h_cfv[n][p][H_p] (counterfactual values), both [n_nodes][H0 + H1] with
  * player 0's hands first.  Either pointer may be NULL.  Synchronous. */
 int mtt_batch_read_vectors(mtt_batch* b, int32_t s, float* h_reach, float* h_cfv);
+/* Root values of subgame s from the last FP64 best-response pass (a solve
+ * with exploitability = 1): h_ev_p[H_p] = counterfactual values of player
+ * p's hands under both average strategies, h_br_p[H_p] = best-response
+ * values against the opponent's average strategy.  Any pointer may be NULL.
+ * Synchronous. */
+int mtt_batch_root_values(mtt_batch* b, int32_t s, double* h_ev0, double* h_ev1, double* h_br0, double* h_br1);
 /* Device bytes held, and algorithmic bytes of one CFR iteration over the whole
  * batch (R,S read+write per action-hand; reach and CFV written and read once
  * per player-hand per node). */
 int mtt_batch_info(mtt_batch* b, int64_t* device_bytes, int64_t* iter_bytes);
+/* Device layout of the per-subgame arrays, for callers that pass their own
+ * strategy inputs: h_rows_off[2*s+p] = float offset of player p's rows block
+ * of subgame s ([rows_p][Hp_p], Hp_p = H_p rounded up to a multiple of 4,
+ * hand i at column i in combos[p] order); h_range_off[s] = float offset of
+ * its packed root ranges [Hp_0 | Hp_1]; totals are the array lengths.  Any
+ * output may be NULL. */
+int mtt_batch_layout(mtt_batch* b, int64_t* h_rows_off, int64_t* h_range_off, int64_t* total_rows,
+                     int64_t* total_range);
+/* Differentiable EV of fixed strategies, no CFR (no reference counterpart;
+ * the values are those of kernel_evaluate_terminals and
+ * kernel_backward_sweep, honest_multistreet_solver.cu:128-249, with card
+ * removal).  Both players play sigma = softmax(logits) over the actions of
+ * every decision node, per hand.  d_logits: [total_rows] in the rows layout;
+ * d_ranges: [total_range] packed root ranges (padding 0).  Outputs:
+ *   d_ev[s]          = EV of player 0 in chips, sum over compatible hand
+ *                      pairs of range0 * range1 * payoff0;
+ *   d_grad_ranges    = dEV0/drange in the range layout: [cfv0 | -cfv1] at the
+ *                      root (the counterfactual values);
+ *   d_grad_logits    = dEV0/dlogits in the rows layout.
+ * All device pointers 16-byte aligned.  Overwrites the batch's per-node
+ * reach and value vectors (a later solve starts from scratch anyway).
+ * Asynchronous; mtt_batch_check reports a bounded-wait failure. */
+int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
+                      float* d_grad_ranges, float* d_grad_logits, void* stream);
+/* Waits for the stream; MTT_ERR_TIMEOUT if a bounded device wait of this
+ * batch's kernels gave up since the last solve or ev_grad started. */
+int mtt_batch_check(mtt_batch* b, void* stream);
 /* Kernels launched for this batch since it was created; a graph replay counts
  * every kernel node it runs. No reference counterpart (instrumentation). */
 int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
@@ -259,6 +292,140 @@ int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
  * batch; *threads receives the choice (also used when params.threads == 0). */
 int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads);
 int mtt_batch_destroy(mtt_batch* b);
+
+/* ------------------------------------------------------ leaf-net GEMM */
+#define MTT_GEMM_RELU     1    /* max(0, .) after the bias */
+#define MTT_GEMM_OUT_BF16 2    /* C is bf16 (else float) */
+#define MTT_GEMM_MASK     4    /* zero C where d_mask (bf16 [M][ldm]) is <= 0: the ReLU backward */
+/* C[M x N] = A[M x K] * B[N x K]^T (+ d_bias[N]) on the tcgen05 tensor cores,
+ * BF16 inputs, FP32 accumulation.  A, B row-major with row strides lda, ldb
+ * (elements, multiples of 8; base addresses 16-byte aligned); C row stride
+ * ldc.  d_err: device int, bit 0 set if a bounded wait gave up.  No
+ * reference counterpart (the reference has no learned component). */
+int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, void* d_C, int32_t ldc,
+                  int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
+                  int32_t flags, int32_t* d_err, void* stream);
+
+/* ------------------------------------------------------ leaf network */
+/* MLP for depth-limited solving (no reference counterpart): features
+ * [ranges of both players over the 1,326 combos | board one-hot (52) | pot |
+ * stack] = 2,706 -> 3 x 1,024 ReLU -> 2,652 counterfactual values (both
+ * players' 1,326 combos, in units of the pot).  BF16 weights and
+ * activations, FP32 accumulation and FP32 master weights (Adam). */
+#define MTT_LEAF_IN     2706
+#define MTT_LEAF_HIDDEN 1024
+#define MTT_LEAF_OUT    2652
+typedef struct mtt_leafnet mtt_leafnet;
+/* batch_cap: largest batch (multiple of 8).  He-initialised from seed. */
+int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, mtt_leafnet** out);
+/* d_x [M][2706] float features -> d_y [M][2652] float predictions. */
+int mtt_leafnet_forward(mtt_leafnet* n, const float* d_x, int32_t M, float* d_y, void* stream);
+/* Gradients of the masked mean squared error sum(w (y - t)^2) / (M * 2652)
+ * for targets d_t [M][2652] and weights d_w (NULL = all ones); *h_loss gets
+ * the loss (synchronises when h_loss is given).  M a multiple of 8. */
+int mtt_leafnet_gradients(mtt_leafnet* n, const float* d_x, const float* d_t, const float* d_w, int32_t M,
+                          double* h_loss, void* stream);
+/* Gradients as above, then one Adam step (beta1 0.9, beta2 0.999, eps 1e-8). */
+int mtt_leafnet_train_step(mtt_leafnet* n, const float* d_x, const float* d_t, const float* d_w, int32_t M,
+                           float lr, double* h_loss, void* stream);
+/* Layer l (0..3) parameters and last gradients in the padded shape
+ * shape[0] x shape[1] = out x in (input 2,752 and output 2,688 columns,
+ * padding zero).  Any pointer may be NULL.  Synchronous. */
+int mtt_leafnet_params(mtt_leafnet* n, int32_t layer, float* h_w, float* h_b, float* h_gw, float* h_gb,
+                       int32_t* shape);
+/* MTT_ERR_TIMEOUT if a bounded wait in the network's GEMMs gave up. */
+int mtt_leafnet_check(mtt_leafnet* n);
+int mtt_leafnet_destroy(mtt_leafnet* n);
+
+/* ------------------------------------------- ICM (Malmuth-Harville, FP64) */
+/* Tournament equity of n seats with chip stacks[n] and m payouts[m] (prize
+ * for 1st, 2nd, ...): the probability that seat i finishes k-th is the
+ * Malmuth-Harville product of stack shares; out[i] = sum_k payouts[k] *
+ * P(i finishes k-th).  n <= 16, m <= n.  Host only.  No reference
+ * counterpart: the reference takes bubble factors as input
+ * (multiway_4way_engine.cu:85, bubble_factors[4x4]). */
+int mtt_icm_equity(const double* stacks, int32_t n, const double* payouts, int32_t m, double* out);
+/* Bubble factors of the players in a hand: seats[k] (k < np <= 4) index the
+ * n seats.  For k != j: risk X = min(stack of k, stack of j);
+ *   bf[k*np + j] = (E_k(now) - E_k(k loses X to j)) / (E_k(k wins X from j) - E_k(now)),
+ * and bf[k*np + k] = the mean of bf[k*np + j] over j != k (k against the
+ * field).  These are the bubble_factors the multiway terminals scale losses
+ * by.  Host only. */
+int mtt_icm_bubble_factors(const double* stacks, int32_t n, const double* payouts, int32_t m,
+                           const int32_t* seats, int32_t np, double* bf);
+
+/* ---------------------------------------------------- multiway (4 players) */
+#define MTT_MW_PLAYERS 4
+#define MTT_MW_MAX_ACTIONS 3   /* as the reference engine (MAX_POST_ACTIONS, multiway_4way_engine.cu:14) */
+/* Flat 4-player node, 32 bytes, the reference's 4-way FlatNode
+ * (multiway_4way_engine.cu:20-24): fold terminals keep the single remaining
+ * player's bit in active_mask; showdown terminals the bits of the players
+ * still in.  As in the heads-up layout, infoset_offset is the first row of
+ * this node in its player's own regret array. */
+typedef struct mtt_mw_node {
+    uint8_t  type;
+    uint8_t  player;
+    uint8_t  num_actions;
+    uint8_t  active_mask;
+    int32_t  children_offset;
+    int32_t  infoset_offset;
+    float    pot_size;
+    float    committed[4];
+} mtt_mw_node;
+
+/* Single-street 4-player betting: players act in seat order 0..3; with no
+ * bet a player checks or bets one of bet_sizes (fractions of the pot); facing
+ * a bet a player folds, calls or (while fewer than raise_cap raises were
+ * made) raises raise_size * (pot + to_call) on top of the call.  Bets are
+ * capped at the player's remaining stack.  The round closes when every
+ * player still in has acted and matched the bet.  At most 3 actions per
+ * node. */
+typedef struct mtt_mw_spec {
+    float   pot;                  /* dead money already in (split equally into committed[]) */
+    float   stacks[4];            /* chips behind per player */
+    int32_t n_bet_sizes;          /* 1 or 2 */
+    float   bet_sizes[2];
+    float   raise_size;
+    int32_t raise_cap;
+} mtt_mw_spec;
+
+int mtt_mw_tree_build(const mtt_mw_spec* spec, mtt_mw_node* nodes, int32_t capacity, int32_t* n_nodes,
+                      int32_t rows[4], int32_t* max_depth);
+
+/* One 4-player river subgame: every player's range is over the same H
+ * ascending combo ids (the reference's shared combo axis), none touching the
+ * board; bubble[16] = loss multipliers bf[p*4 + w] (row p loses to w; the
+ * diagonal is p against the field), 1 = chip EV. */
+typedef struct mtt_mw_subgame {
+    const mtt_mw_node* nodes;
+    int32_t n_nodes;
+    int32_t rows[4];
+    uint8_t board[5];
+    int32_t H;
+    const uint16_t* combos;
+    const float* ranges[4];
+    float bubble[16];
+} mtt_mw_subgame;
+
+typedef struct mtt_mw_batch mtt_mw_batch;
+
+int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw_batch** out);
+/* CFR+ (or DCFR) with simultaneous updates of all four players, as the
+ * reference kernels (kernel_4way_forward_sweep / _evaluate_terminals /
+ * _backward_cfr_plus, multiway_4way_engine.cu:41-257).  Uses iters, algo,
+ * alpha/beta/gamma, semantics (MTT_SEM_REFERENCE: the reference's strict
+ * rank-position order, no ties; MTT_SEM_CORRECT: equal hands split the pot),
+ * avg_power; one iteration is captured as a CUDA graph when graph != 0.
+ * Neither semantics removes cards between the players' hands (the reference
+ * does not).  Asynchronous. */
+int mtt_mw_batch_solve(mtt_mw_batch* b, const mtt_solve_params* prm, int32_t graph, void* stream);
+/* Per subgame and player, the EV of that player's range (chips) under the
+ * average strategies: h_out[s*4 + p].  Synchronous. */
+int mtt_mw_batch_values(mtt_mw_batch* b, double* h_out, void* stream);
+/* R_p, S_p ([rows_p][H]) and the last iteration's root CFVs ([4][H]) of
+ * subgame s; any pointer may be NULL.  Synchronous. */
+int mtt_mw_batch_read(mtt_mw_batch* b, int32_t s, float* h_R[4], float* h_S[4], float* h_cfv);
+int mtt_mw_batch_destroy(mtt_mw_batch* b);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

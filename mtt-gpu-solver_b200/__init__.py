@@ -139,6 +139,38 @@ def board_showdown_counts(board, hands, stream=None):
     return W, T, L_
 
 
+GEMM_RELU, GEMM_OUT_BF16, GEMM_MASK = 1, 2, 4
+
+
+def gemm_bf16(A, B, bias=None, relu=False, out_bf16=False, mask=None, out=None, err=None, stream=None):
+    """C = A @ B.T (+ bias, ReLU / ReLU-mask) on the tcgen05 tensor cores.
+    A: bf16 CUDA [M, K], B: bf16 CUDA [N, K] (row-major, K contiguous, row
+    strides multiples of 8); C: float32 or bf16 [M, N]."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    if out is None:
+        out = torch.empty((M, N), dtype=torch.bfloat16 if out_bf16 else torch.float32, device=A.device)
+    own_err = err is None
+    if own_err:
+        err = torch.zeros(1, dtype=torch.int32, device=A.device)
+    flags = (GEMM_RELU if relu else 0) | (GEMM_OUT_BF16 if out_bf16 else 0) | (GEMM_MASK if mask is not None else 0)
+    for t in (A, B):
+        if t.dtype != torch.bfloat16 or not t.is_cuda or t.stride(1) != 1:
+            raise TypeError("A and B must be bf16 CUDA matrices with unit column stride")
+    check("mtt_gemm_bf16", lib().mtt_gemm_bf16(
+        ctypes.c_void_p(A.data_ptr()), A.stride(0), ctypes.c_void_p(B.data_ptr()), B.stride(0),
+        ctypes.c_void_p(out.data_ptr()), out.stride(0), M, N, K,
+        _dev(bias, torch.float32) if bias is not None else None,
+        ctypes.c_void_p(mask.data_ptr()) if mask is not None else None, mask.stride(0) if mask is not None else 0,
+        flags, ctypes.c_void_p(err.data_ptr()), _stream(stream)))
+    if own_err:
+        torch.cuda.current_stream().synchronize() if stream is None else None
+        if int(err.item()):
+            raise MttError("mtt_gemm_bf16", 4)
+    return out
+
+
 def canonical_flops():
     out = np.zeros(1755 * 4, dtype=np.uint8)
     n = ctypes.c_int32()
@@ -212,6 +244,7 @@ class RiverBatch:
         self.n = len(subgames)
         self.meta = [(int(g["rows"][0]), int(g["rows"][1]), len(g["combos0"]), len(g["combos1"]))
                      for g in subgames]
+        self.combos = [(np.asarray(g["combos0"], np.int64), np.asarray(g["combos1"], np.int64)) for g in subgames]
         h = ctypes.c_void_p()
         check("mtt_batch_create", lib().mtt_batch_create(arr, len(subgames), ctypes.byref(h)))
         self._h = h
@@ -249,11 +282,46 @@ class RiverBatch:
         check("mtt_batch_read_vectors", lib().mtt_batch_read_vectors(self._h, s, reach.ctypes.data, cfv.ctypes.data))
         return reach, cfv
 
+    def root_values(self, s):
+        """FP64 root values of subgame s from the last best-response pass:
+        (ev0, ev1, br0, br1), each over that player's combos."""
+        rows0, rows1, H0, H1 = self.meta[s]
+        out = [np.zeros(H0), np.zeros(H1), np.zeros(H0), np.zeros(H1)]
+        check("mtt_batch_root_values", lib().mtt_batch_root_values(self._h, s, *[o.ctypes.data for o in out]))
+        return tuple(out)
+
     def info(self):
         db = ctypes.c_int64()
         ib = ctypes.c_int64()
         check("mtt_batch_info", lib().mtt_batch_info(self._h, ctypes.byref(db), ctypes.byref(ib)))
         return {"device_bytes": db.value, "iter_bytes": ib.value}
+
+    def layout(self):
+        """Offsets of each subgame's rows blocks and packed ranges in the
+        device layout (see mtt_batch_layout)."""
+        rows_off = np.zeros((self.n, 2), np.int64)
+        range_off = np.zeros(self.n, np.int64)
+        tr, tg = ctypes.c_int64(), ctypes.c_int64()
+        check("mtt_batch_layout", lib().mtt_batch_layout(self._h, rows_off.ctypes.data, range_off.ctypes.data,
+                                                         ctypes.byref(tr), ctypes.byref(tg)))
+        return {"rows_off": rows_off, "range_off": range_off, "total_rows": tr.value, "total_range": tg.value}
+
+    def ev_grad(self, logits, ranges, stream=None):
+        """EV of player 0 under softmax(logits) strategies and its gradients.
+        logits: float32 CUDA [total_rows], ranges: float32 CUDA [total_range]
+        (layout()).  Returns (ev [n], grad_ranges, grad_logits), CUDA float32."""
+        import torch
+        ev = torch.empty(self.n, dtype=torch.float32, device=logits.device)
+        g_r = torch.empty_like(ranges)
+        g_l = torch.empty_like(logits)
+        check("mtt_batch_ev_grad", lib().mtt_batch_ev_grad(
+            self._h, _dev(logits, torch.float32), _dev(ranges, torch.float32), _dev(ev, torch.float32),
+            _dev(g_r, torch.float32), _dev(g_l, torch.float32), _stream(stream)))
+        return ev, g_r, g_l
+
+    def check(self, stream=None):
+        """Waits for the stream; raises if a bounded device wait gave up."""
+        check("mtt_batch_check", lib().mtt_batch_check(self._h, _stream(stream)))
 
     def launch_count(self):
         """Kernels launched for this batch so far (graph replays count every node)."""

@@ -49,6 +49,24 @@ class Subgame(ctypes.Structure):
                 ("combos", ctypes.c_void_p * 2), ("ranges", ctypes.c_void_p * 2)]
 
 
+MW_NODE_DTYPE = np.dtype([
+    ("type", "u1"), ("player", "u1"), ("num_actions", "u1"), ("active_mask", "u1"),
+    ("children_offset", "<i4"), ("infoset_offset", "<i4"), ("pot_size", "<f4"), ("committed", "<f4", (4,)),
+])
+assert MW_NODE_DTYPE.itemsize == 32
+
+
+class MwSpec(ctypes.Structure):
+    _fields_ = [("pot", ctypes.c_float), ("stacks", ctypes.c_float * 4), ("n_bet_sizes", ctypes.c_int32),
+                ("bet_sizes", ctypes.c_float * 2), ("raise_size", ctypes.c_float), ("raise_cap", ctypes.c_int32)]
+
+
+class MwSubgame(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int32), ("rows", ctypes.c_int32 * 4),
+                ("board", ctypes.c_uint8 * 5), ("H", ctypes.c_int32), ("combos", ctypes.c_void_p),
+                ("ranges", ctypes.c_void_p * 4), ("bubble", ctypes.c_float * 16)]
+
+
 class MttError(RuntimeError):
     def __init__(self, fn, status, cuda_err=0):
         super().__init__(f"{fn} failed: {STATUS.get(status, status)} (status {status}, cudaError {cuda_err})")
@@ -88,7 +106,27 @@ def lib():
         "mtt_batch_iterations": ([vp, vp], ctypes.c_int),
         "mtt_batch_read_vectors": ([vp, i32, vp, vp], ctypes.c_int),
         "mtt_batch_info": ([vp, vp, vp], ctypes.c_int),
+        "mtt_batch_root_values": ([vp, i32, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_launch_count": ([vp, vp], ctypes.c_int),
+        "mtt_batch_layout": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_ev_grad": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_check": ([vp, vp], ctypes.c_int),
+        "mtt_gemm_bf16": ([vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp, i32, i32, vp, vp], ctypes.c_int),
+        "mtt_leafnet_create": ([i32, ctypes.c_uint64, vp], ctypes.c_int),
+        "mtt_leafnet_forward": ([vp, vp, i32, vp, vp], ctypes.c_int),
+        "mtt_leafnet_gradients": ([vp, vp, vp, vp, i32, vp, vp], ctypes.c_int),
+        "mtt_leafnet_train_step": ([vp, vp, vp, vp, i32, ctypes.c_float, vp, vp], ctypes.c_int),
+        "mtt_leafnet_params": ([vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_leafnet_check": ([vp], ctypes.c_int),
+        "mtt_leafnet_destroy": ([vp], ctypes.c_int),
+        "mtt_icm_equity": ([vp, i32, vp, i32, vp], ctypes.c_int),
+        "mtt_icm_bubble_factors": ([vp, i32, vp, i32, vp, i32, vp], ctypes.c_int),
+        "mtt_mw_tree_build": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_mw_batch_create": ([vp, i32, vp], ctypes.c_int),
+        "mtt_mw_batch_solve": ([vp, vp, i32, vp], ctypes.c_int),
+        "mtt_mw_batch_values": ([vp, vp, vp], ctypes.c_int),
+        "mtt_mw_batch_read": ([vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_mw_batch_destroy": ([vp], ctypes.c_int),
         "mtt_batch_autotune": ([vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_destroy": ([vp], ctypes.c_int),
     }

@@ -1,0 +1,251 @@
+// gemm.cu — BF16 GEMM on the 5th-generation tensor cores (tcgen05) for the
+// leaf network: C[M x N] = epilogue(A[M x K] * B[N x K]^T), A and B row-major
+// (K contiguous), FP32 accumulation in tensor memory.
+//
+// One 128 x 128 output tile per CTA of 192 threads:
+//   warp 0      one thread streams 128 x 64 tiles of A and B into a 4-stage
+//               shared-memory ring with 2-D TMA loads (128-byte swizzle),
+//               completing on the stage's "full" mbarrier;
+//   warp 1      allocates 128 TMEM columns; one thread issues
+//               tcgen05.mma (M=128, N=128, K=16, kind::f16, BF16 in, FP32
+//               accumulate) four times per stage and commits each stage back
+//               to its "empty" mbarrier, then commits the accumulator;
+//   warps 2..5  read the accumulator with tcgen05.ld (warp w owns TMEM lanes
+//               32*(w%4) .. +31 = output rows), add the bias, apply ReLU or a
+//               ReLU mask, convert and store.
+// Every mbarrier wait is bounded; a wait that gives up sets *err, the
+// producer still waits (bounded) for its own copies and the allocating warp
+// frees the TMEM before the CTA leaves.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "mtt_bulk.cuh"
+#include "mtt_common.h"
+
+namespace mtt {
+namespace gemm {
+
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4, THREADS = 192;
+constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // tiles (1024-aligned) + barriers
+constexpr uint32_t TMEM_COLS = 128;
+
+enum { F_RELU = 1, F_OUT_BF16 = 2, F_MASK = 4 };
+
+// Shared-memory matrix descriptor of a K-major operand tile written by TMA
+// with 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart (stride
+// byte offset), leading byte offset 16 B (unused for swizzled K-major),
+// descriptor version 1, layout type 2 = SWIZZLE_128B.
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+    const uint64_t a = (uint64_t)(smem_addr(p) >> 4) & 0x3FFFull;
+    return a | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor of kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
+// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    const uint32_t m0 = 0u, m1 = 0u, m2 = 0u, m3 = 0u;   // no output lanes disabled
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2), "r"(m3)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, void* __restrict__ C,
+            int M, int N, int K, int ldc, const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
+            int ldm, int flags, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accum = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+    int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int KT = (K + BK - 1) / BK;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(accum, 1);
+        *s_fail = 0;
+        mbar_fence_init();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // producer: stage s of k-tile kt; the stage is free once the MMAs of
+        // k-tile kt - STAGES have completed (their commit to empty[s])
+        int kt = 0;
+        for (; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES && !mbar_wait_bounded(&empty[s], (uint32_t)((kt / STAGES - 1) & 1))) {
+                atomicOr(err, 1);
+                *s_fail = 1;
+                break;
+            }
+            uint8_t* st = smem + s * STAGE_BYTES;
+            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            tma_load_2d(st, &ta, kt * BK, m0, &full[s]);
+            tma_load_2d(st + A_BYTES, &tb, kt * BK, n0, &full[s]);
+        }
+        // our own copies have landed before the CTA can leave
+        for (int j = (kt > STAGES ? kt - STAGES : 0); j < kt; ++j)
+            (void)mbar_wait_bounded(&full[j % STAGES], (uint32_t)((j / STAGES) & 1));
+    } else if (warp == 1 && lane == 0) {
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait_bounded(&full[s], (uint32_t)((kt / STAGES) & 1))) {
+                atomicOr(err, 1);
+                *s_fail = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint8_t* st = smem + s * STAGE_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+                umma_bf16(tmem, smem_desc(st + kk * 32), smem_desc(st + A_BYTES + kk * 32), (kt | kk) ? 1u : 0u);
+            umma_commit(&empty[s]);
+        }
+        umma_commit(accum);   // fires when every MMA issued above has completed
+    } else if (warp >= 2) {
+        const bool ok = mbar_wait_bounded(accum, 0u);
+        __syncwarp();
+        tc_fence_after();
+        if (!ok) atomicOr(err, 1);
+        const int lg = warp & 3;                     // TMEM lanes 32*lg .. 32*lg+31
+        const int row = m0 + 32 * lg + lane;
+        const bool live = ok && !*(volatile int*)s_fail;
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)c, r);
+            if (!live || row >= M) continue;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = n0 + c + j;
+                if (col >= N) break;
+                float v = __uint_as_float(r[j]);
+                if (bias) v += bias[col];
+                if ((flags & F_RELU) && v < 0.0f) v = 0.0f;
+                if ((flags & F_MASK) && !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f)) v = 0.0f;
+                if (flags & F_OUT_BF16) reinterpret_cast<__nv_bfloat16*>(C)[(size_t)row * ldc + col] = __float2bfloat16_rn(v);
+                else reinterpret_cast<float*>(C)[(size_t)row * ldc + col] = v;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// Host: the driver's tensor-map encoder, found once through the runtime.
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::once_flag g_encode_once;
+
+static int encoder(PFN_cuTensorMapEncodeTiled_v12000* out) {
+    std::call_once(g_encode_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!g_encode) return MTT_ERR_UNSUPPORTED;
+    *out = g_encode;
+    return MTT_OK;
+}
+
+// 2-D map of a row-major bf16 matrix [rows x cols] with leading dimension ld,
+// box 64 (cols) x 128 (rows), 128-byte swizzle, zero fill outside.
+static int make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc;
+    MTT_TRY(encoder(&enc));
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MTT_OK : MTT_ERR_INVALID;
+}
+
+static int launch(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
+                  const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st) {
+    if (M <= 0 || N <= 0 || K <= 0) return M == 0 || N == 0 ? MTT_OK : MTT_ERR_INVALID;
+    if (!A || !B || !C || !d_err || (lda % 8) || (ldb % 8) || lda < K || ldb < K || ldc < N) return MTT_ERR_INVALID;
+    if (((uintptr_t)A & 15) || ((uintptr_t)B & 15)) return MTT_ERR_INVALID;
+    if ((flags & F_MASK) && (!mask || ldm < N)) return MTT_ERR_INVALID;
+    CUtensorMap ta, tb;
+    MTT_TRY(make_map(&ta, A, M, K, lda));
+    MTT_TRY(make_map(&tb, B, N, K, ldb));
+    MTT_TRY_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    k_gemm_bf16<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, C, M, N, K, ldc, bias,
+                                                    reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err);
+    MTT_CHECK_LAUNCH();
+    return MTT_OK;
+}
+
+}  // namespace gemm
+
+int gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
+              const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st) {
+    return gemm::launch(A, lda, B, ldb, C, ldc, M, N, K, bias, mask, ldm, flags, d_err, st);
+}
+
+}  // namespace mtt
+
+extern "C" int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, void* d_C, int32_t ldc,
+                             int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
+                             int32_t flags, int32_t* d_err, void* stream) {
+    return mtt::gemm_bf16(d_A, lda, d_B, ldb, d_C, ldc, M, N, K, d_bias, d_mask, ldm, flags, d_err,
+                          mtt::as_stream(stream));
+}

@@ -1,15 +1,17 @@
 // mtt_bulk.cuh — mbarrier + cp.async.bulk (TMA 1-D bulk copy) helpers for sm_100a.
 //
 // Only plain, non-multicast global->shared bulk copies of this GPU's own
-// memory are issued.  Every wait is bounded: after MTT_WAIT_LIMIT polls the
-// caller gets `false`, records an error word and leaves.
+// memory are issued.  Every wait is bounded: after MTT_WAIT_LIMIT polls or
+// MTT_WAIT_NS of wall time (%globaltimer) the caller gets `false`, records an
+// error word and leaves.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace mtt {
 
-constexpr uint32_t MTT_WAIT_LIMIT = 1u << 24;
+constexpr uint32_t MTT_WAIT_LIMIT = 1u << 24;          // polls
+constexpr uint64_t MTT_WAIT_NS = 2000000000ull;       // and at most 2 s of wall time per wait
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -50,9 +52,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0u;
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < MTT_WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 0; i < MTT_WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 63u && globaltimer_ns() - t0 > MTT_WAIT_NS) return false;
+    }
     return false;
 }
 

@@ -139,14 +139,14 @@ __device__ __forceinline__ TermInfo term_info(const SubDesc& sd, const DNode& nd
 __host__ __device__ constexpr int term_scratch(int max_h) { return 4 * max_h + 96; }
 constexpr int TT = 128;   // threads per terminal CTA (fixed: results never depend on it changing)
 
-template <typename TA>
+template <typename TA, int NT = TT>
 __device__ __forceinline__ TA cta_sum(TA v, TA* wb, int tid) {
     v = warp_sum(v);
     if ((tid & 31) == 0) wb[tid >> 5] = v;
     __syncthreads();
     TA t = TA(0);
 #pragma unroll
-    for (int k = 0; k < TT / 32; ++k) t += wb[k];
+    for (int k = 0; k < NT / 32; ++k) t += wb[k];
     __syncthreads();
     return t;
 }
@@ -159,8 +159,9 @@ __device__ __forceinline__ TA cta_sum(TA v, TA* wb, int tid) {
 // exactly zero (all of the opponent's remaining mass blocked by the hand's
 // cards) must come out as zero to the precision the regret-matching
 // threshold (1e-7) can see.  X: the CTA's shared scratch (term_scratch
-// elements), wb: 8 elements.
-template <typename TI, typename TA, typename TO, bool STAGED = false>
+// elements), wb: NT/32 elements.  NT: threads of the CTA; the scan's chunks
+// depend on it, so each caller fixes it.
+template <typename TI, typename TA, typename TO, bool STAGED = false, int NT = TT>
 __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const TI* __restrict__ ro,
                              TO* __restrict__ out, TO* __restrict__ out2, TA* X, TA* wb, int semantics, int tid) {
     const int o = 1 - q;
@@ -176,7 +177,7 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     TA* Xs = STAGED ? X : X + Ho + 8;   // scan region (3*Ho + 1) / fold: per-card order + card sums
     if (!STAGED) {
 #pragma unroll 4
-        for (int j = tid; j < Ho; j += TT) Rd[j] = (TA)ro[j];
+        for (int j = tid; j < Ho; j += NT) Rd[j] = (TA)ro[j];
         __syncthreads();
     }
     auto Rs = [&](int j) -> TA { return STAGED ? (TA)ro[j] : Rd[j]; };
@@ -184,19 +185,19 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         const int winner = (ti.wmask == 1) ? 0 : 1;
         const TA payoff = (q == winner) ? gain : loss;
         TA part = TA(0);
-        for (int j = tid; j < Ho; j += TT) part += Rs(j);
-        const TA tot = cta_sum(part, wb, tid);
+        for (int j = tid; j < Ho; j += NT) part += Rs(j);
+        const TA tot = cta_sum<TA, NT>(part, wb, tid);
         TA* Cs = Xs + 2 * Ho + 8;
 #pragma unroll 4
-        for (int e = tid; e < 2 * Ho; e += TT) Xs[e] = Rs(co[e]);
+        for (int e = tid; e < 2 * Ho; e += NT) Xs[e] = Rs(co[e]);
         __syncthreads();
-        for (int c = tid; c < 52; c += TT) {
+        for (int c = tid; c < 52; c += NT) {
             TA sm = TA(0);
             for (int e = seg[c]; e < seg[c + 1]; ++e) sm += Xs[e];
             Cs[c] = sm;
         }
         __syncthreads();
-        for (int h = tid; h < Hpq; h += TT) {
+        for (int h = tid; h < Hpq; h += NT) {
             TA v = TA(0);
             if (h < Hq) {
                 const Entry et = ent[h];
@@ -216,9 +217,9 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     const uint16_t* so = tv.sorted[o];
     const int N = 3 * Ho;
 #pragma unroll 4
-    for (int k = tid; k < N; k += TT) Xs[k] = Rs(k < Ho ? so[k] : co[k - Ho]);
+    for (int k = tid; k < N; k += NT) Xs[k] = Rs(k < Ho ? so[k] : co[k - Ho]);
     __syncthreads();
-    const int C = ((N + TT - 1) / TT) | 1;   // odd chunk: conflict-free strides
+    const int C = ((N + NT - 1) / NT) | 1;   // odd chunk: conflict-free strides
     const int s0 = min(tid * C, N), s1 = min(s0 + C, N);
     TA loc = TA(0);
     for (int k = s0; k < s1; ++k) loc += Xs[k];
@@ -235,7 +236,7 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     __syncthreads();
     TA base = TA(0), total = TA(0);
 #pragma unroll
-    for (int k = 0; k < TT / 32; ++k) {
+    for (int k = 0; k < NT / 32; ++k) {
         if (k < wid) base += wb[k];
         total += wb[k];
     }
@@ -248,7 +249,7 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     if (tid == 0) Xs[N] = total;
     __syncthreads();
     const TA Tt = Xs[Ho];
-    for (int h = tid; h < Hpq; h += TT) {
+    for (int h = tid; h < Hpq; h += NT) {
         TA v = TA(0);
         if (h < Hq) {
             const Entry et = ent[h];
@@ -298,11 +299,12 @@ struct alignas(16) BwdItem {    // 64 B
     long long child;      // arena float offset (CFV region) of child 0's part for player q
     long long self;       // arena float offset (CFV region) of this node's part for q
     long long rows;       // R float offset of the node's first row (update items)
-    long long hc;         // hand-card offset of q (chance items)
+    long long hc;         // hand-card offset of q (chance items); q's reach at the node (BI_SUMS items)
     int h4;
     int hs4;
     int na;
-    int flags;            // BI_UPDATE: q acts here; BI_CHANCE; otherwise sum of children
+    int flags;            // BI_UPDATE: q acts here (BI_SUMS: also add to S); BI_CHANCE; else sum of children;
+                          // BI_NEG: q == 1 (sign of dEV0 in the differentiable pass)
     int first;            // global index of child 0 (chance items)
     float div;            // chance divisor
     int g0;               // first float4 group of this warp
@@ -320,7 +322,7 @@ struct alignas(16) TermItem {   // 80 B
 };
 static_assert(sizeof(FwdItem) == 64 && sizeof(BwdItem) == 64 && sizeof(TermItem) == 96, "item sizes");
 enum { FI_REACH = 1, FI_SUMS = 2, FI_CHANCE = 4 };
-enum { BI_UPDATE = 1, BI_CHANCE = 4 };
+enum { BI_UPDATE = 1, BI_SUMS = 2, BI_CHANCE = 4, BI_NEG = 8 };
 
 __global__ void k_init(SolveDev a, int n_sub) {
     const int s = blockIdx.x;
@@ -342,6 +344,81 @@ __global__ void k_init(SolveDev a, int n_sub) {
 
 __global__ void k_next_iter(SolveDev a) {
     if (threadIdx.x == 0) *a.iter += 1;
+}
+
+// Fixed-action-count paths of the sweeps: every row of the node is loaded
+// before any is used (A independent 16-byte loads in flight per lane), with
+// the same operations in the same order as the general loops below, so the
+// results are bit-identical.
+template <int A>
+__device__ __forceinline__ void fwd_reach_fixed(const float4* __restrict__ Rb, const float4* __restrict__ rp,
+                                                float4* __restrict__ ch, int H4, int HS4, int g) {
+    float4 rk[A];
+#pragma unroll
+    for (int k = 0; k < A; ++k) rk[k] = max04(Rb[(size_t)k * H4 + g]);
+    const float4 r = rp[g];
+    float4 sum = f4(0.f);
+#pragma unroll
+    for (int k = 0; k < A; ++k) sum = add4(sum, rk[k]);
+    const float invA = __fdiv_rn(1.0f, (float)A);
+#pragma unroll
+    for (int k = 0; k < A; ++k) ch[(size_t)k * HS4 + g] = mul4(r, rm4(rk[k], sum, invA));
+}
+
+template <int A>
+__device__ __forceinline__ void bwd_sum_fixed(const float4* __restrict__ qc, float4* __restrict__ out, int HS4, int g) {
+    float4 qk[A];
+#pragma unroll
+    for (int k = 0; k < A; ++k) qk[k] = qc[(size_t)k * HS4 + g];
+    float4 so = f4(0.f);
+#pragma unroll
+    for (int k = 0; k < A; ++k) so = add4(so, qk[k]);
+    out[g] = so;
+}
+
+template <int A>
+__device__ __forceinline__ void bwd_update_fixed(float4* __restrict__ Rb, float4* __restrict__ Sb,
+                                                 const float4* __restrict__ qc, const float4* __restrict__ rr,
+                                                 float4* __restrict__ out, int H4, int HS4, int g, bool ds, bool dcfr,
+                                                 float4 tb) {
+    float4 rk[A], qk[A];
+#pragma unroll
+    for (int k = 0; k < A; ++k) { rk[k] = Rb[(size_t)k * H4 + g]; qk[k] = qc[(size_t)k * HS4 + g]; }
+    const float invA = __fdiv_rn(1.0f, (float)A);
+    float4 sum = f4(0.f);
+#pragma unroll
+    for (int k = 0; k < A; ++k) sum = add4(sum, max04(rk[k]));
+    float4 v = f4(0.f);
+#pragma unroll
+    for (int k = 0; k < A; ++k) v = fma4(rm4(max04(rk[k]), sum, invA), qk[k], v);
+    out[g] = v;
+    if (ds) {
+        const float4 r = rr[g];
+        const float4 wr = mul4(r, f4(tb.x));
+#pragma unroll
+        for (int k = 0; k < A; ++k) {
+            const float4 sg = rm4(max04(rk[k]), sum, invA);
+            float4 sv = Sb[(size_t)k * H4 + g];
+            sv = dcfr ? fma4(r, sg, mul4(sv, f4(tb.w))) : fma4(wr, sg, sv);
+            Sb[(size_t)k * H4 + g] = sv;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < A; ++k) {
+        float4 nr;
+        if (dcfr) {
+            nr.x = dcfr1(rk[k].x, __fsub_rn(qk[k].x, v.x), tb.y, tb.z);
+            nr.y = dcfr1(rk[k].y, __fsub_rn(qk[k].y, v.y), tb.y, tb.z);
+            nr.z = dcfr1(rk[k].z, __fsub_rn(qk[k].z, v.z), tb.y, tb.z);
+            nr.w = dcfr1(rk[k].w, __fsub_rn(qk[k].w, v.w), tb.y, tb.z);
+        } else {
+            nr.x = cfrplus1(rk[k].x, __fsub_rn(qk[k].x, v.x));
+            nr.y = cfrplus1(rk[k].y, __fsub_rn(qk[k].y, v.y));
+            nr.z = cfrplus1(rk[k].z, __fsub_rn(qk[k].z, v.z));
+            nr.w = cfrplus1(rk[k].w, __fsub_rn(qk[k].w, v.w));
+        }
+        Rb[(size_t)k * H4 + g] = nr;
+    }
 }
 
 // Forward sweep of one level: regret matching, children's reach and/or
@@ -376,6 +453,18 @@ __global__ void __launch_bounds__(256, 3) k_fwd(SolveDev a, const FwdItem* __res
     const bool dr = it.flags & FI_REACH, ds = it.flags & FI_SUMS;
     const float4* Rb = reinterpret_cast<const float4*>(a.R + it.rows);
     float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
+    if (dr && !ds) {
+        const int g = it.g0 + lane;
+        if (g >= H4) return;
+        switch (A) {
+            case 2: fwd_reach_fixed<2>(Rb, rp, ch, H4, HS4, g); return;
+            case 3: fwd_reach_fixed<3>(Rb, rp, ch, H4, HS4, g); return;
+            case 4: fwd_reach_fixed<4>(Rb, rp, ch, H4, HS4, g); return;
+            case 5: fwd_reach_fixed<5>(Rb, rp, ch, H4, HS4, g); return;
+            case 6: fwd_reach_fixed<6>(Rb, rp, ch, H4, HS4, g); return;
+            default: break;
+        }
+    }
     const float invA = __fdiv_rn(1.0f, (float)A);
     float w_lin = 0.f, dstr = 0.f;
     if (ds) {
@@ -404,69 +493,152 @@ __global__ void __launch_bounds__(256, 3) k_fwd(SolveDev a, const FwdItem* __res
     }
 }
 
-// Shared memory of one staged terminal direction: the opponent's reach
-// (FP32), the opponent's index block, this player's entry block and the FP64
-// scan region.
-__host__ __device__ inline int term_stage_bytes(int Hpo, int Ho, int Hq) {
-    // FP64 region: showdown scan 3*Ho + 1, fold per-card order 2*Ho + card sums at 2*Ho + 8 .. + 52
-    const int xd = (3 * Ho + 8) > (2 * Ho + 64) ? (3 * Ho + 8) : (2 * Ho + 64);
-    return 4 * Hpo + tab_idx_bytes(Ho) + tab_ent_bytes(Hq) + 8 * xd + 64;
+// Terminals are processed in groups: consecutive terminals of one subgame
+// that share a showdown table variant (all of a river subgame's terminals,
+// or those below one river card of a turn subgame), at most TG_CHUNK per
+// CTA.  The CTA stages the table blocks once, then walks its terminals with
+// the opponent reach of terminal t+1 in flight (1-D bulk copy on the other
+// stage's mbarrier) while terminal t is evaluated from shared memory.
+constexpr int TG = 256;         // threads per terminal-group CTA (fixed: the scan chunks depend on it)
+constexpr int TG_CHUNK = 16;    // terminals per group at most
+
+struct alignas(16) TermGroup {  // 32 B
+    long long tab;              // byte offset of the table variant
+    int first, count;           // items [first, first + count) of the terminal list
+    int H0, H1, Hp0, Hp1;
+};
+static_assert(sizeof(TermGroup) == 32, "TermGroup is 32 bytes");
+
+// Shared-memory plan of a group for the updated players `upd` (bit q = q's
+// values are computed).  One direction (upd = 1 << q) needs the opponent's
+// index block, q's entry block and the opponent's reach; both directions
+// need the whole variant and both reach vectors.
+__host__ __device__ inline int tg_table_bytes(int H0, int H1, int upd) {
+    if (upd == 3) return tab_variant_bytes(H0, H1);
+    const int q = upd == 1 ? 0 : 1;
+    const int Ho = q ? H0 : H1, Hq = q ? H1 : H0;
+    return tab_idx_bytes(Ho) + tab_ent_bytes(Hq);
+}
+__host__ __device__ inline int tg_reach_bytes(int Hp0, int Hp1, int upd) {
+    return upd == 3 ? 4 * (Hp0 + Hp1) : 4 * (upd == 1 ? Hp1 : Hp0);
+}
+__host__ __device__ inline int tg_scan_doubles(int H0, int H1, int upd) {
+    int m = 0;
+    for (int q = 0; q < 2; ++q) {
+        if (!((upd >> q) & 1)) continue;
+        const int Ho = q ? H0 : H1;
+        const int need = (3 * Ho + 8) > (2 * Ho + 64) ? (3 * Ho + 8) : (2 * Ho + 64);
+        m = need > m ? need : m;
+    }
+    return m;
+}
+__host__ __device__ inline int tg_smem_bytes(int H0, int H1, int Hp0, int Hp1, int upd) {
+    return tg_table_bytes(H0, H1, upd) + 2 * tg_reach_bytes(Hp0, Hp1, upd) + 8 * tg_scan_doubles(H0, H1, upd) + 16;
 }
 
-// Terminal values of the updated players, one CTA per terminal
-// (kernel_evaluate_terminals, honest_multistreet_solver.cu:128-196).  Thread 0
-// stages the opponent's reach, the opponent's rank/card index block and this
-// player's entry block into shared memory with three 1-D bulk copies on one
-// mbarrier; the CTA then works from shared memory only.
-__global__ void __launch_bounds__(TT) k_term(SolveDev a, const TermItem* __restrict__ items, int n, int upd) {
+// Terminal values of the updated players (kernel_evaluate_terminals,
+// honest_multistreet_solver.cu:128-196), one terminal group per CTA.
+__global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __restrict__ groups,
+                                             const TermItem* __restrict__ items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ double wb[8];
-    const int w = blockIdx.x, tid = threadIdx.x;
-    if (w >= n) return;
-    const TermItem it = items[w];
+    __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s
+    __shared__ double wb[TG / 32];
+    const int gi = blockIdx.x, tid = threadIdx.x;
+    if (gi >= n) return;
+    const TermGroup g = groups[gi];
+    const bool both = upd == 3;
+    const int q1 = upd == 2 ? 1 : 0;            // the updated player of a one-direction launch
+    const uint32_t tb = (uint32_t)tg_table_bytes(g.H0, g.H1, upd);
+    const uint32_t rbytes = (uint32_t)tg_reach_bytes(g.Hp0, g.Hp1, upd);
+    uint8_t* T = smem;
+    float* Rst0 = reinterpret_cast<float*>(smem + tb);
+    float* Rst1 = reinterpret_cast<float*>(smem + tb + rbytes);
+    double* X = reinterpret_cast<double*>(smem + tb + 2 * rbytes);   // tb, rbytes: multiples of 16
     if (tid == 0) {
-        mbar_init(&bar, 1);
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
         mbar_fence_init();
     }
     __syncthreads();
-    uint32_t parity = 0u;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        if (!((upd >> q) & 1)) continue;
-        const int o = 1 - q;
-        const int Ho = it.H[o], Hpo = it.Hp[o], Hq = it.H[q];
-        const uint32_t rb = 4u * (uint32_t)Hpo, ib = (uint32_t)tab_idx_bytes(Ho), eb = (uint32_t)tab_ent_bytes(Hq);
-        float* Ro = reinterpret_cast<float*>(smem);
-        uint8_t* Ib = smem + rb;
-        uint8_t* Eb = Ib + ib;
-        double* X = reinterpret_cast<double*>(Eb + eb);   // rb, ib, eb are multiples of 16
-        if (tid == 0) {
-            mbar_arrive_expect_tx(&bar, rb + ib + eb);
-            bulk_g2s(Ro, a.arena + it.ro[o], rb, &bar);
-            bulk_g2s(Ib, a.tabs + it.tab + tab_idx_off(o, it.H[0]), ib, &bar);
-            bulk_g2s(Eb, a.tabs + it.tab + tab_ent_off(q, it.H[0], it.H[1]), eb, &bar);
+    // thread 0 issues every copy; stage s of terminal t is reach vector(s) of items[first + t]
+    auto issue_reach = [&](int t, int s) {
+        const TermItem& it = items[g.first + t];
+        float* dst = s ? Rst1 : Rst0;
+        mbar_arrive_expect_tx(&bar[1 + s], rbytes);
+        if (both) {
+            bulk_g2s(dst, a.arena + it.ro[0], 4u * (uint32_t)g.Hp0, &bar[1 + s]);
+            bulk_g2s(dst + g.Hp0, a.arena + it.ro[1], 4u * (uint32_t)g.Hp1, &bar[1 + s]);
+        } else {
+            bulk_g2s(dst, a.arena + it.ro[1 - q1], rbytes, &bar[1 + s]);
         }
-        const bool ok = mbar_wait_bounded(&bar, parity);
-        parity ^= 1u;
+    };
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&bar[0], tb);
+        if (both) {
+            bulk_g2s(T, a.tabs + g.tab, tb, &bar[0]);
+        } else {
+            const int o = 1 - q1;
+            const int Ho = o ? g.H1 : g.H0;
+            const uint32_t ib = (uint32_t)tab_idx_bytes(Ho);
+            bulk_g2s(T, a.tabs + g.tab + tab_idx_off(o, g.H0), ib, &bar[0]);
+            bulk_g2s(T + ib, a.tabs + g.tab + tab_ent_off(q1, g.H0, g.H1), tb - ib, &bar[0]);
+        }
+        issue_reach(0, 0);
+    }
+    const bool okt = mbar_wait_bounded(&bar[0], 0u);
+    if (__syncthreads_or(!okt)) {
+        if (tid == 0) atomicOr(a.err, 1);
+        (void)mbar_wait_bounded(&bar[1], 0u);    // the first reach copy may still be in flight
+        return;
+    }
+    TabView tv;
+    if (both) {
+        tv = tab_view(T, g.H0, g.H1);
+    } else {
+        // one direction: both slots get the staged blocks (only the opponent's
+        // index slot and q's entry slot are read), so no slot is chosen at run time
+        const int Ho = q1 ? g.H0 : g.H1;
+        const uint16_t *so, *co, *sg;
+        tab_idx_view(T, Ho, &so, &co, &sg);
+        const Entry* en = reinterpret_cast<const Entry*>(T + tab_idx_bytes(Ho));
+        tv.sorted[0] = tv.sorted[1] = so;
+        tv.cl[0] = tv.cl[1] = co;
+        tv.seg[0] = tv.seg[1] = sg;
+        tv.ent[0] = tv.ent[1] = en;
+    }
+    TermInfo ti;
+    ti.H[0] = g.H0; ti.H[1] = g.H1; ti.Hp[0] = g.Hp0; ti.Hp[1] = g.Hp1;
+    uint32_t parity = 0u;   // bit s: phase of stage s
+    for (int t = 0; t < g.count; ++t) {
+        const int s = t & 1;
+        // stage s ^ 1 was last read by terminal t - 1, which ended on a barrier
+        if (tid == 0 && t + 1 < g.count) issue_reach(t + 1, s ^ 1);
+        const bool ok = mbar_wait_bounded(&bar[1 + s], (parity >> s) & 1u);
+        parity ^= 1u << s;
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(a.err, 1);
+            if (t + 1 < g.count) (void)mbar_wait_bounded(&bar[2 - s], (parity >> (s ^ 1)) & 1u);
             return;
         }
-        TabView tv;
-        tab_idx_view(Ib, Ho, &tv.sorted[o], &tv.cl[o], &tv.seg[o]);
-        tv.ent[q] = reinterpret_cast<const Entry*>(Eb);
-        TermInfo ti;
-        ti.H[0] = it.H[0]; ti.H[1] = it.H[1]; ti.Hp[0] = it.Hp[0]; ti.Hp[1] = it.Hp[1];
+        const TermItem& it = items[g.first + t];
         ti.pot = it.pot; ti.c[0] = it.c0; ti.c[1] = it.c1;
         ti.type = it.type_wmask & 0xFF; ti.wmask = (it.type_wmask >> 8) & 0xFF;
-        cta_terminal<float, double, float, true>(ti, tv, q, Ro, a.arena + it.out[q], nullptr, X, wb, a.semantics, tid);
+        const float* st = s ? Rst1 : Rst0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (!((upd >> q) & 1)) continue;
+            // opponent reach: player 1's part follows player 0's in a two-direction stage
+            const float* ro = both ? (q == 0 ? st + g.Hp0 : st) : st;
+            cta_terminal<float, double, float, true, TG>(ti, tv, q, ro, a.arena + it.out[q], nullptr, X, wb,
+                                                         a.semantics, tid);
+        }
     }
 }
 
 // Backward sweep of one level for the updated players: counterfactual values
 // and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
-__global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+__global__ void __launch_bounds__(256, 2) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
@@ -497,6 +669,14 @@ __global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __res
     const int g = it.g0 + lane;
     if (g >= H4) return;
     if (!(it.flags & BI_UPDATE)) {
+        switch (A) {
+            case 2: bwd_sum_fixed<2>(qc, out, HS4, g); return;
+            case 3: bwd_sum_fixed<3>(qc, out, HS4, g); return;
+            case 4: bwd_sum_fixed<4>(qc, out, HS4, g); return;
+            case 5: bwd_sum_fixed<5>(qc, out, HS4, g); return;
+            case 6: bwd_sum_fixed<6>(qc, out, HS4, g); return;
+            default: break;
+        }
         {
             float4 so = f4(0.f);
             for (int k = 0; k < A; ++k) so = add4(so, qc[(size_t)k * HS4 + g]);
@@ -506,20 +686,51 @@ __global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __res
     }
     const float invA = __fdiv_rn(1.0f, (float)A);
     float4* Rb = reinterpret_cast<float4*>(a.R + it.rows);
-    float dpos = 0.f, dneg = 0.f;
+    float dpos = 0.f, dneg = 0.f, w_lin = 0.f, dstr = 0.f;
     const bool dcfr = a.algo == MTT_ALGO_DCFR;
-    if (dcfr) {
+    const bool ds = it.flags & BI_SUMS;
+    if (dcfr || ds) {
         const float4 tb = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (*a.iter - 1));
         dpos = tb.y;
         dneg = tb.z;
+        w_lin = tb.x;
+        dstr = tb.w;
+    }
+    {
+        const float4 tb = make_float4(w_lin, dpos, dneg, dstr);
+        float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
+        const float4* rr = reinterpret_cast<const float4*>(a.arena + it.hc);
+        switch (A) {
+            case 2: bwd_update_fixed<2>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
+            case 3: bwd_update_fixed<3>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
+            case 4: bwd_update_fixed<4>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
+            case 5: bwd_update_fixed<5>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
+            case 6: bwd_update_fixed<6>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
+            default: break;
+        }
     }
     // Rows and child values are re-read (L1 hits) instead of held in registers.
     {
         float4 sum = f4(0.f);
         for (int k = 0; k < A; ++k) sum = add4(sum, max04(Rb[(size_t)k * H4 + g]));
         float4 v = f4(0.f);
-        for (int k = 0; k < A; ++k)
-            v = fma4(rm4(max04(Rb[(size_t)k * H4 + g]), sum, invA), qc[(size_t)k * HS4 + g], v);
+        if (ds) {
+            // strategy sums of the acting player, from the same sigma and with
+            // the same arithmetic as the forward sweep's FI_SUMS path
+            const float4 r = reinterpret_cast<const float4*>(a.arena + it.hc)[g];
+            const float4 wr = mul4(r, f4(w_lin));
+            float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
+            for (int k = 0; k < A; ++k) {
+                const float4 sg = rm4(max04(Rb[(size_t)k * H4 + g]), sum, invA);
+                v = fma4(sg, qc[(size_t)k * HS4 + g], v);
+                float4 sv = Sb[(size_t)k * H4 + g];
+                sv = dcfr ? fma4(r, sg, mul4(sv, f4(dstr))) : fma4(wr, sg, sv);
+                Sb[(size_t)k * H4 + g] = sv;
+            }
+        } else {
+            for (int k = 0; k < A; ++k)
+                v = fma4(rm4(max04(Rb[(size_t)k * H4 + g]), sum, invA), qc[(size_t)k * HS4 + g], v);
+        }
         out[g] = v;
         for (int k = 0; k < A; ++k) {
             const float4 rk = Rb[(size_t)k * H4 + g];
@@ -539,6 +750,149 @@ __global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __res
             Rb[(size_t)k * H4 + g] = nr;
         }
     }
+}
+
+// ------------------------------------------------------------- differentiable EV
+// Fixed strategies sigma = softmax(logits) per node and hand; the logits sit
+// in the regret layout (a.R) and dEV0/dlogits is written in the same layout
+// (a.S).  One forward pass (reach), the terminals of both players and one
+// backward pass (counterfactual values and the adjoint of the softmax) give
+// EV0 and all its gradients: dEV0/drange0 = cfv0 at the root, dEV0/drange1 =
+// -cfv1 at the root (zero-sum payoffs), and for a node of player p
+//   dEV0/dlogit_a(h) = sgn_p * reach_p(h) * sigma_a(h) * (cfv_p(child a, h) - cfv_p(node, h)),
+// sgn_0 = +1, sgn_1 = -1.
+__device__ __forceinline__ void softmax_groups(const float4* Lb, int H4, int g, int A, float4& mx, float4& den) {
+    mx = Lb[g];
+    for (int k = 1; k < A; ++k) {
+        const float4 l = Lb[(size_t)k * H4 + g];
+        mx = make_float4(fmaxf(mx.x, l.x), fmaxf(mx.y, l.y), fmaxf(mx.z, l.z), fmaxf(mx.w, l.w));
+    }
+    den = f4(0.f);
+    for (int k = 0; k < A; ++k) {
+        const float4 l = Lb[(size_t)k * H4 + g];
+        den = add4(den, make_float4(expf(l.x - mx.x), expf(l.y - mx.y), expf(l.z - mx.z), expf(l.w - mx.w)));
+    }
+}
+__device__ __forceinline__ float4 softmax_at(const float4* Lb, int H4, int g, int k, float4 mx, float4 den) {
+    const float4 l = Lb[(size_t)k * H4 + g];
+    return make_float4(__fdiv_rn(expf(l.x - mx.x), den.x), __fdiv_rn(expf(l.y - mx.y), den.y),
+                       __fdiv_rn(expf(l.z - mx.z), den.z), __fdiv_rn(expf(l.w - mx.w), den.w));
+}
+
+__global__ void k_ev_init(SolveDev a, int n_sub) {
+    const int s = blockIdx.x;
+    if (s == 0 && threadIdx.x == 0) *a.err = 0;
+    if (s >= n_sub) return;
+    const SubDesc sd = a.desc[s];
+    const int HS4 = (sd.Hp0 + sd.Hp1) >> 2;
+    const float4* rg = reinterpret_cast<const float4*>(a.ranges + sd.range_base);
+    float4* rr = reinterpret_cast<float4*>(a.arena + sd.arena_base);
+    for (int i = threadIdx.x; i < HS4; i += blockDim.x) rr[i] = rg[i];
+}
+
+// Forward level: children's reach under softmax strategies; chance items as k_fwd.
+__global__ void __launch_bounds__(256) k_ev_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const FwdItem it = items[w];
+    const float4* rp = reinterpret_cast<const float4*>(a.arena + it.reach_in);
+    float4* ch = reinterpret_cast<float4*>(a.arena + it.child);
+    const int A = it.na, H4 = it.h4, HS4 = it.hs4;
+    const int g = it.g0 + lane;
+    if (g >= H4) return;
+    if (it.flags & FI_CHANCE) {
+        const uint16_t* hc = a.hcards + it.hc;
+        const float4 r = rp[g];
+        const uint64_t m0 = hand_mask(hc[4 * g]), m1 = hand_mask(hc[4 * g + 1]);
+        const uint64_t m2 = hand_mask(hc[4 * g + 2]), m3 = hand_mask(hc[4 * g + 3]);
+        for (int k = 0; k < A; ++k) {
+            const int card = a.nodes[it.first + k].dealt;
+            float4 v = r;
+            if ((m0 >> card) & 1ull) v.x = 0.f;
+            if ((m1 >> card) & 1ull) v.y = 0.f;
+            if ((m2 >> card) & 1ull) v.z = 0.f;
+            if ((m3 >> card) & 1ull) v.w = 0.f;
+            ch[(size_t)k * HS4 + g] = v;
+        }
+        return;
+    }
+    const float4* Lb = reinterpret_cast<const float4*>(a.R + it.rows);
+    float4 mx, den;
+    softmax_groups(Lb, H4, g, A, mx, den);
+    const float4 r = rp[g];
+    for (int k = 0; k < A; ++k) ch[(size_t)k * HS4 + g] = mul4(r, softmax_at(Lb, H4, g, k, mx, den));
+}
+
+// Backward level: values of both players; the acting player's items also
+// write the logit gradient.
+__global__ void __launch_bounds__(256) k_ev_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const BwdItem it = items[w];
+    const float4* qc = reinterpret_cast<const float4*>(a.arena + it.child);
+    float4* out = reinterpret_cast<float4*>(a.arena + it.self);
+    const int A = it.na, H4 = it.h4, HS4 = it.hs4;
+    const int g = it.g0 + lane;
+    if (g >= H4) return;
+    if (it.flags & BI_CHANCE) {
+        const uint16_t* hc = a.hcards + it.hc;
+        const float dv = it.div;
+        const uint64_t m0 = hand_mask(hc[4 * g]), m1 = hand_mask(hc[4 * g + 1]);
+        const uint64_t m2 = hand_mask(hc[4 * g + 2]), m3 = hand_mask(hc[4 * g + 3]);
+        float4 acc = f4(0.f);
+        for (int k = 0; k < A; ++k) {
+            const int card = a.nodes[it.first + k].dealt;
+            const float4 cv = qc[(size_t)k * HS4 + g];
+            if (!((m0 >> card) & 1ull)) acc.x = __fadd_rn(acc.x, cv.x);
+            if (!((m1 >> card) & 1ull)) acc.y = __fadd_rn(acc.y, cv.y);
+            if (!((m2 >> card) & 1ull)) acc.z = __fadd_rn(acc.z, cv.z);
+            if (!((m3 >> card) & 1ull)) acc.w = __fadd_rn(acc.w, cv.w);
+        }
+        out[g] = make_float4(__fdiv_rn(acc.x, dv), __fdiv_rn(acc.y, dv), __fdiv_rn(acc.z, dv), __fdiv_rn(acc.w, dv));
+        return;
+    }
+    if (!(it.flags & BI_UPDATE)) {
+        float4 so = f4(0.f);
+        for (int k = 0; k < A; ++k) so = add4(so, qc[(size_t)k * HS4 + g]);
+        out[g] = so;
+        return;
+    }
+    const float4* Lb = reinterpret_cast<const float4*>(a.R + it.rows);
+    float4* Gb = reinterpret_cast<float4*>(a.S + it.rows);
+    float4 mx, den;
+    softmax_groups(Lb, H4, g, A, mx, den);
+    float4 v = f4(0.f);
+    for (int k = 0; k < A; ++k) v = fma4(softmax_at(Lb, H4, g, k, mx, den), qc[(size_t)k * HS4 + g], v);
+    out[g] = v;
+    const float4 r = reinterpret_cast<const float4*>(a.arena + it.hc)[g];
+    const float sgn = it.flags & BI_NEG ? -1.0f : 1.0f;
+    const float4 sr = mul4(r, f4(sgn));
+    for (int k = 0; k < A; ++k) {
+        const float4 sg = softmax_at(Lb, H4, g, k, mx, den);
+        const float4 d = make_float4(__fsub_rn(qc[(size_t)k * HS4 + g].x, v.x), __fsub_rn(qc[(size_t)k * HS4 + g].y, v.y),
+                                     __fsub_rn(qc[(size_t)k * HS4 + g].z, v.z), __fsub_rn(qc[(size_t)k * HS4 + g].w, v.w));
+        Gb[(size_t)k * H4 + g] = mul4(mul4(sr, sg), d);
+    }
+}
+
+// Root: EV0 = sum_h range0(h) cfv0(root, h) (accumulated in FP64), and the
+// range gradients [cfv0 | -cfv1] in the packed range layout.
+__global__ void __launch_bounds__(TT) k_ev_root(SolveDev a, int n_sub, float* __restrict__ ev,
+                                               float* __restrict__ grad_ranges) {
+    __shared__ double wb[TT / 32];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    if (s >= n_sub) return;
+    const SubDesc sd = a.desc[s];
+    const int HS = sd.Hp0 + sd.Hp1;
+    const float* cf = a.arena + sd.arena_base + (size_t)sd.n_nodes * HS;
+    const float* rg = a.ranges + sd.range_base;
+    double acc = 0.0;
+    for (int h = tid; h < sd.H0; h += TT) acc += (double)rg[h] * (double)cf[h];
+    for (int i = tid; i < HS; i += TT) grad_ranges[sd.range_base + i] = i < sd.Hp0 ? cf[i] : -cf[i];
+    acc = cta_sum(acc, wb, tid);
+    if (tid == 0) ev[s] = (float)acc;
 }
 
 // ------------------------------------------------------------- FP64 best response
@@ -755,7 +1109,7 @@ struct HostLists {
     std::vector<std::vector<FwdItem>> fi, fsim, fal[2];
     std::vector<std::vector<BwdItem>> bsim, bal[2];
     std::vector<std::vector<Task>> bf, bb;
-    std::vector<TermItem> titems;    // ascending hand count
+    std::vector<TermItem> titems;    // by subgame, then table variant
     std::vector<int2> terms;
 };
 
@@ -768,7 +1122,10 @@ struct ListSet {
     int2* terms = nullptr;
     long long terms_cap = 0;
     int n_terms = 0;
-    std::vector<int> tb_start, tb_count, tb_smem;   // terminal buckets: offset, size, shared bytes
+    TermGroup* tgroups = nullptr;
+    long long tgroups_cap = 0;
+    std::vector<int> tb_start, tb_count;             // terminal-group buckets: offset, size
+    std::vector<int> tb_smem1, tb_smem3;             // shared bytes: one direction / both
     int* subs = nullptr;
     long long subs_cap = 0;
     int n_subs = 0;
@@ -823,6 +1180,7 @@ static void free_set(ListSet& L) {
     cudaFree(L.f_init.d); cudaFree(L.f_sim.d); cudaFree(L.b_sim.d);
     for (int u = 0; u < 2; ++u) { cudaFree(L.f_alt[u].d); cudaFree(L.b_alt[u].d); }
     cudaFree(L.br_fwd.d); cudaFree(L.br_bwd.d); cudaFree(L.titems); cudaFree(L.terms); cudaFree(L.subs);
+    cudaFree(L.tgroups);
 }
 
 static void free_batch(mtt_batch* b) {
@@ -893,22 +1251,47 @@ static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, 
     if (!subs.empty()) MTT_TRY_CUDA(cudaMemcpy(L.subs, subs.data(), sizeof(int) * subs.size(), cudaMemcpyHostToDevice));
     L.n_terms = (int)tm.size();
     L.n_subs = (int)subs.size();
-    // terminal buckets: ascending hand count, three equal-count launches whose
-    // shared memory is sized by their largest terminal
-    L.tb_start.clear(); L.tb_count.clear(); L.tb_smem.clear();
-    const int nt = (int)ti.size(), nb = nt < 3 ? 1 : 3;
+    // Terminal groups: runs of items with the same subgame and table variant
+    // (the host list is ordered that way), cut into chunks of TG_CHUNK.
+    std::vector<TermGroup> gr;
+    for (int i = 0; i < (int)ti.size();) {
+        int j = i + 1;
+        while (j < (int)ti.size() && j - i < TG_CHUNK && ti[j].sub == ti[i].sub && ti[j].tab == ti[i].tab) ++j;
+        TermGroup g{};
+        g.tab = ti[i].tab;
+        g.first = i;
+        g.count = j - i;
+        g.H0 = ti[i].H[0]; g.H1 = ti[i].H[1]; g.Hp0 = ti[i].Hp[0]; g.Hp1 = ti[i].Hp[1];
+        gr.push_back(g);
+        i = j;
+    }
+    // Buckets: ascending hand count, three equal-count launches whose shared
+    // memory is sized by their largest group; inside a bucket the costliest
+    // groups go first so that the last wave is made of short ones.
+    std::stable_sort(gr.begin(), gr.end(), [](const TermGroup& x, const TermGroup& y) {
+        return std::max(x.Hp0, x.Hp1) < std::max(y.Hp0, y.Hp1);
+    });
+    L.tb_start.clear(); L.tb_count.clear(); L.tb_smem1.clear(); L.tb_smem3.clear();
+    const int ng = (int)gr.size(), nb = ng < 3 ? 1 : 3;
     for (int k = 0; k < nb; ++k) {
-        const int lo = (int)((long long)nt * k / nb), hi = (int)((long long)nt * (k + 1) / nb);
-        int need = 0;
+        const int lo = (int)((long long)ng * k / nb), hi = (int)((long long)ng * (k + 1) / nb);
+        std::stable_sort(gr.begin() + lo, gr.begin() + hi, [](const TermGroup& x, const TermGroup& y) {
+            return (long long)x.count * (x.H0 + x.H1) > (long long)y.count * (y.H0 + y.H1);
+        });
+        int need1 = 0, need3 = 0;
         for (int i = lo; i < hi; ++i) {
-            const TermItem& t = ti[i];
-            need = std::max(need, term_stage_bytes(t.Hp[1], t.H[1], t.H[0]));
-            need = std::max(need, term_stage_bytes(t.Hp[0], t.H[0], t.H[1]));
+            const TermGroup& g = gr[i];
+            need1 = std::max(need1, tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 1));
+            need1 = std::max(need1, tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 2));
+            need3 = std::max(need3, tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 3));
         }
         L.tb_start.push_back(lo);
         L.tb_count.push_back(hi - lo);
-        L.tb_smem.push_back(need);
+        L.tb_smem1.push_back(need1);
+        L.tb_smem3.push_back(need3);
     }
+    MTT_TRY(grow(&L.tgroups, &L.tgroups_cap, (long long)gr.size(), total));
+    if (!gr.empty()) MTT_TRY_CUDA(cudaMemcpy(L.tgroups, gr.data(), sizeof(TermGroup) * gr.size(), cudaMemcpyHostToDevice));
     return MTT_OK;
 }
 
@@ -975,7 +1358,8 @@ static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelL
 static int launch_term(const mtt_batch* b, const ListSet& L, const SolveDev& a, int upd, cudaStream_t st) {
     for (size_t k = 0; k < L.tb_start.size(); ++k) {
         if (L.tb_count[k] == 0) continue;
-        k_term<<<L.tb_count[k], TT, L.tb_smem[k], st>>>(a, L.titems + L.tb_start[k], L.tb_count[k], upd);
+        const int smem = upd == 3 ? L.tb_smem3[k] : L.tb_smem1[k];
+        k_term<<<L.tb_count[k], TG, smem, st>>>(a, L.tgroups + L.tb_start[k], L.titems, L.tb_count[k], upd);
         MTT_CHECK_LAUNCH();
         ++b->launches;
     }
@@ -1041,7 +1425,8 @@ static int set_smem_attrs(const mtt_batch* b, const ListSet& L) {
         MTT_TRY_CUDA(cudaFuncSetAttribute(k_br_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t));
     }
     int tmax = 0;
-    for (int v : L.tb_smem) tmax = std::max(tmax, v);
+    for (int v : L.tb_smem1) tmax = std::max(tmax, v);
+    for (int v : L.tb_smem3) tmax = std::max(tmax, v);
     if (tmax > 48 * 1024) MTT_TRY_CUDA(cudaFuncSetAttribute(k_term, cudaFuncAttributeMaxDynamicSharedMemorySize, tmax));
     return MTT_OK;
 }
@@ -1229,7 +1614,9 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                 for (f.g0 = 0; f.g0 < f.h4; f.g0 += 32) {
                     f.flags = FI_REACH; HL.fi[dp].push_back(f);
                     f.flags = FI_REACH | FI_SUMS; HL.fsim[dp].push_back(f);
-                    for (int u = 0; u < 2; ++u) { f.flags = (p == u) ? FI_SUMS : FI_REACH; HL.fal[u][dp].push_back(f); }
+                    // alternating pass u: the opponent's nodes pass reach down; the
+                    // acting player's strategy sums are added by its backward items
+                    f.flags = FI_REACH; HL.fal[1 - p][dp].push_back(f);
                 }
                 for (int q = 0; q < 2; ++q) {
                     BwdItem bw{};
@@ -1239,10 +1626,12 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     bw.h4 = H4[q];
                     bw.hs4 = (int)(HS / 4);
                     bw.na = nd.na;
-                    bw.flags = q == p ? BI_UPDATE : 0;
                     bw.sub = i;
+                    bw.hc = q == p ? f.reach_in : 0;
                     for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
+                        bw.flags = q == p ? (BI_UPDATE | (q ? BI_NEG : 0)) : 0;
                         HL.bsim[dp].push_back(bw);
+                        if (q == p) bw.flags = BI_UPDATE | BI_SUMS;
                         HL.bal[q][dp].push_back(bw);
                     }
                 }
@@ -1302,8 +1691,9 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
             }
         }
     }
+    // terminals of one subgame and table variant are contiguous (terminal groups)
     std::stable_sort(HL.titems.begin(), HL.titems.end(), [](const TermItem& x, const TermItem& y) {
-        return std::max(x.Hp[0], x.Hp[1]) < std::max(y.Hp[0], y.Hp[1]);
+        return x.sub != y.sub ? x.sub < y.sub : x.tab < y.tab;
     });
     long long total = 0;
     int s = MTT_OK;
@@ -1419,11 +1809,91 @@ extern "C" int mtt_batch_read_vectors(mtt_batch* b, int32_t s, float* h_reach, f
     return MTT_OK;
 }
 
+extern "C" int mtt_batch_root_values(mtt_batch* b, int32_t s, double* h_ev0, double* h_ev1, double* h_br0,
+                                     double* h_br1) {
+    if (!b || s < 0 || s >= b->n) return MTT_ERR_INVALID;
+    MTT_TRY_CUDA(cudaDeviceSynchronize());
+    const SubDesc& d = b->desc[s];
+    const size_t HS = (size_t)d.Hp0 + d.Hp1, reg = ((size_t)d.n_nodes + 1) * HS;
+    const double* br = b->d_darena + d.darena_base + reg;
+    const double* ev = br + reg;
+    if (h_ev0) MTT_TRY_CUDA(cudaMemcpy(h_ev0, ev, sizeof(double) * d.H0, cudaMemcpyDeviceToHost));
+    if (h_ev1) MTT_TRY_CUDA(cudaMemcpy(h_ev1, ev + d.Hp0, sizeof(double) * d.H1, cudaMemcpyDeviceToHost));
+    if (h_br0) MTT_TRY_CUDA(cudaMemcpy(h_br0, br, sizeof(double) * d.H0, cudaMemcpyDeviceToHost));
+    if (h_br1) MTT_TRY_CUDA(cudaMemcpy(h_br1, br + d.Hp0, sizeof(double) * d.H1, cudaMemcpyDeviceToHost));
+    return MTT_OK;
+}
+
 extern "C" int mtt_batch_info(mtt_batch* b, int64_t* device_bytes, int64_t* iter_bytes) {
     if (!b) return MTT_ERR_INVALID;
     if (device_bytes) *device_bytes = b->device_bytes;
     if (iter_bytes) *iter_bytes = b->iter_bytes;
     return MTT_OK;
+}
+
+extern "C" int mtt_batch_layout(mtt_batch* b, int64_t* h_rows_off, int64_t* h_range_off, int64_t* total_rows,
+                                int64_t* total_range) {
+    if (!b) return MTT_ERR_INVALID;
+    long long tr = 0, tg = 0;
+    for (int i = 0; i < b->n; ++i) {
+        const SubDesc& d = b->desc[i];
+        if (h_rows_off) { h_rows_off[2 * i] = d.rs_base0; h_rows_off[2 * i + 1] = d.rs_base1; }
+        if (h_range_off) h_range_off[i] = d.range_base;
+        tr = std::max(tr, d.rs_base1 + (long long)d.rows1 * d.Hp1);
+        tg = std::max(tg, d.range_base + (long long)(d.Hp0 + d.Hp1));
+    }
+    if (total_rows) *total_rows = tr;
+    if (total_range) *total_range = tg;
+    return MTT_OK;
+}
+
+extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
+                                 float* d_grad_ranges, float* d_grad_logits, void* stream) {
+    auto al16 = [](const void* p) { return p && ((uintptr_t)p & 15u) == 0; };
+    if (!b || !al16(d_logits) || !al16(d_ranges) || !d_ev || !al16(d_grad_ranges) || !al16(d_grad_logits))
+        return MTT_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    mtt_solve_params p{};
+    p.algo = MTT_ALGO_CFRPLUS;
+    p.semantics = MTT_SEM_CORRECT;
+    SolveDev a = dev_args(b, p);
+    a.R = const_cast<float*>(d_logits);
+    a.S = d_grad_logits;
+    a.ranges = d_ranges;
+    const ListSet& L = b->full;
+    MTT_TRY(set_smem_attrs(b, L));
+    k_ev_init<<<b->n, 256, 0, st>>>(a, b->n);
+    MTT_CHECK_LAUNCH();
+    ++b->launches;
+    const long long warps = 256 / 32;
+    for (int d = 0; d < b->levels; ++d) {
+        const long long n = L.f_init.off[d + 1] - L.f_init.off[d];
+        if (n == 0) continue;
+        k_ev_fwd<<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.f_init.d + L.f_init.off[d], (int)n);
+        MTT_CHECK_LAUNCH();
+        ++b->launches;
+    }
+    MTT_TRY(launch_term(b, L, a, 3, st));
+    for (int d = b->levels - 1; d >= 0; --d) {
+        const long long n = L.b_sim.off[d + 1] - L.b_sim.off[d];
+        if (n == 0) continue;
+        k_ev_bwd<<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.b_sim.d + L.b_sim.off[d], (int)n);
+        MTT_CHECK_LAUNCH();
+        ++b->launches;
+    }
+    k_ev_root<<<b->n, TT, 0, st>>>(a, b->n, d_ev, d_grad_ranges);
+    MTT_CHECK_LAUNCH();
+    ++b->launches;
+    return MTT_OK;
+}
+
+extern "C" int mtt_batch_check(mtt_batch* b, void* stream) {
+    if (!b) return MTT_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    int err = 0;
+    MTT_TRY_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MTT_TRY_CUDA(cudaStreamSynchronize(st));
+    return err ? MTT_ERR_TIMEOUT : MTT_OK;
 }
 
 extern "C" int mtt_batch_launch_count(mtt_batch* b, int64_t* launches) {

@@ -58,7 +58,7 @@ struct alignas(16) SubDesc {
 //   IDX0 = u16 sorted0[H0] | u16 cl0[2*H0] | u16 seg0[54]      (opponent lists of player 0)
 //   IDX1 = the same for player 1
 //   ENT0 = Entry e0[H0] (player-0 hands against player-1 lists), ENT1 = Entry e1[H1]
-struct Entry {
+struct alignas(4) Entry {   // 4-byte aligned: read as three 32-bit words
     uint8_t c1, c2, ltc1, lec1, ltc2, lec2;
     uint16_t lt, le;     // lt == 0xFFFF: hand blocked by the dealt card
     int16_t same;        // opponent index of the same combo, -1 if absent

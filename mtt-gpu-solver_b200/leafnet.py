@@ -1,0 +1,176 @@
+"""The leaf network: an MLP (2,706 -> 3 x 1,024 ReLU -> 2,652) that predicts
+both players' river counterfactual values, trained on the GPU by the
+library's own tcgen05 GEMM forward and backward kernels (C ABI wrappers).
+
+Features of a river subgame (features()): each player's range over the
+1,326 combos normalised to sum 1 and scaled by the number of live combos,
+the board as a 52-card one-hot, pot / 100 and stack / 100.  Targets: the
+root counterfactual values of each combo divided by the pot (ranges summing
+to 1), zero and weight 0 for combos that touch the board."""
+import ctypes
+
+import numpy as np
+
+from . import combo_cards
+from ._lib import check, lib
+
+IN, HIDDEN, OUT = 2706, 1024, 2652
+
+
+def _stream(s):
+    if s is None:
+        return None
+    return ctypes.c_void_p(s.cuda_stream if hasattr(s, "cuda_stream") else int(s))
+
+
+def features(board, range0_1326, range1_1326, pot, stack):
+    """One feature row (float32 [2706]) from full 1,326-combo ranges."""
+    x = np.zeros(IN, np.float32)
+    live = np.ones(1326, bool)
+    for c in board:
+        live &= ~np.any(_CARDS == int(c), axis=1)
+    n_live = int(live.sum())
+    for p, r in enumerate((range0_1326, range1_1326)):
+        r = np.asarray(r, np.float64) * live
+        s = r.sum()
+        x[p * 1326:(p + 1) * 1326] = (r / s * n_live if s > 0 else r).astype(np.float32)
+    for c in board:
+        x[2652 + int(c)] = 1.0
+    x[2704] = pot / 100.0
+    x[2705] = stack / 100.0
+    return x
+
+
+_CARDS = np.array([(a, b) for a in range(52) for b in range(a + 1, 52)], np.int64)
+
+
+class LeafNet:
+    def __init__(self, batch_cap=4096, seed=0):
+        h = ctypes.c_void_p()
+        check("mtt_leafnet_create", lib().mtt_leafnet_create(int(batch_cap), int(seed), ctypes.byref(h)))
+        self._h = h
+        self.cap = batch_cap
+
+    @staticmethod
+    def _ptr(t, n_cols):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+                and t.dim() == 2 and t.shape[1] == n_cols):
+            raise TypeError(f"expected a contiguous CUDA float32 [M, {n_cols}] tensor")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def forward(self, x, stream=None):
+        import torch
+        y = torch.empty((x.shape[0], OUT), dtype=torch.float32, device=x.device)
+        check("mtt_leafnet_forward", lib().mtt_leafnet_forward(self._h, self._ptr(x, IN), x.shape[0],
+                                                               ctypes.c_void_p(y.data_ptr()), _stream(stream)))
+        return y
+
+    def gradients(self, x, t, w=None, stream=None):
+        loss = ctypes.c_double()
+        check("mtt_leafnet_gradients", lib().mtt_leafnet_gradients(
+            self._h, self._ptr(x, IN), self._ptr(t, OUT), self._ptr(w, OUT) if w is not None else None, x.shape[0],
+            ctypes.byref(loss), _stream(stream)))
+        return loss.value
+
+    def train_step(self, x, t, w=None, lr=1e-3, stream=None, want_loss=True):
+        loss = ctypes.c_double()
+        check("mtt_leafnet_train_step", lib().mtt_leafnet_train_step(
+            self._h, self._ptr(x, IN), self._ptr(t, OUT), self._ptr(w, OUT) if w is not None else None, x.shape[0],
+            float(lr), ctypes.byref(loss) if want_loss else None, _stream(stream)))
+        return loss.value if want_loss else None
+
+    def params(self, layer):
+        shape = (ctypes.c_int32 * 2)()
+        check("mtt_leafnet_params", lib().mtt_leafnet_params(self._h, layer, None, None, None, None, shape))
+        o, i = shape[0], shape[1]
+        w = np.zeros((o, i), np.float32); b = np.zeros(o, np.float32)
+        gw = np.zeros((o, i), np.float32); gb = np.zeros(o, np.float32)
+        check("mtt_leafnet_params", lib().mtt_leafnet_params(self._h, layer, w.ctypes.data, b.ctypes.data,
+                                                             gw.ctypes.data, gb.ctypes.data, shape))
+        return {"w": w, "b": b, "gw": gw, "gb": gb}
+
+    def check(self):
+        check("mtt_leafnet_check", lib().mtt_leafnet_check(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mtt_leafnet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _live_mask(board):
+    live = np.ones(1326, bool)
+    for c in board:
+        live &= ~np.any(_CARDS == int(c), axis=1)
+    return live
+
+
+def river_training_set(n, seed=0, iters=300, batch=2048, spr=(0.5, 1.0, 2.0, 3.0, 4.0), stream=None):
+    """n solver-generated training samples.  Each is a river subgame on a
+    seeded board with pot 100, stack 100 * SPR (SPR from `spr`), bets {50%,
+    100%} + all-in and one raise, ranges Dirichlet(alpha) over the live
+    combos (alpha ~ U[0.1, 1] per player), solved by the batched GPU solver
+    (alternating CFR+, quadratic averaging, `iters` iterations); the targets
+    are the FP64 root values of both players under the average strategies,
+    divided by the pot.  Returns (X [n,2706], T [n,2652], W [n,2652], meta)."""
+    from . import RiverBatch, build_tree, solve_params
+    rng = np.random.default_rng(seed)
+    trees = {s: build_tree(100.0, 100.0 * s, [0.5, 1.0], raise_cap=1) for s in spr}
+    X = np.zeros((n, IN), np.float32)
+    T = np.zeros((n, OUT), np.float32)
+    W = np.zeros((n, OUT), np.float32)
+    meta = []
+    for b0 in range(0, n, batch):
+        subs = []
+        for _ in range(min(batch, n - b0)):
+            board = [int(c) for c in rng.choice(52, size=5, replace=False)]
+            live = np.nonzero(_live_mask(board))[0]
+            s = float(rng.choice(spr))
+            nodes, rows, _ = trees[s]
+            g = {"nodes": nodes, "rows": rows, "board": board, "pot": 100.0, "stack": 100.0 * s}
+            for p in range(2):
+                w = rng.dirichlet(np.full(len(live), rng.uniform(0.1, 1.0)))
+                g[f"combos{p}"] = live.astype(np.uint16)
+                g[f"range{p}"] = (w / w.sum()).astype(np.float32)
+            subs.append(g)
+        rb = RiverBatch(subs)
+        rb.solve(solve_params(iters=iters, exploitability=True, alternate=True, avg_power=2.0), graph=True,
+                 stream=stream)
+        for k, g in enumerate(subs):
+            i = b0 + k
+            ev0, ev1, _, _ = rb.root_values(k)
+            full = [np.zeros(1326), np.zeros(1326)]
+            for p, ev in enumerate((ev0, ev1)):
+                c = g[f"combos{p}"].astype(np.int64)
+                full[p][c] = g[f"range{p}"]
+                T[i, p * 1326 + c] = (ev / g["pot"]).astype(np.float32)
+                W[i, p * 1326 + c] = 1.0
+            X[i] = features(g["board"], full[0], full[1], g["pot"], g["stack"])
+            meta.append({"board": g["board"], "range0": full[0], "range1": full[1]})
+        rb.close()
+    return X, T, W, meta
+
+
+def checkdown_values(meta, device="cuda"):
+    """The leaf estimate without a network: both players check the river
+    down; per combo 0.5 * sum_j r_opp(j) (win - loss) in units of the pot,
+    from the GPU showdown counts.  Returns [n, 2652] like the targets."""
+    import torch
+    from . import board_showdown_counts
+    hands = torch.from_numpy(_CARDS.astype(np.uint8)).to(device)
+    out = np.zeros((len(meta), OUT), np.float32)
+    for i, m in enumerate(meta):
+        Wc, Tc, Lc = board_showdown_counts(torch.tensor(m["board"], dtype=torch.uint8, device=device), hands)
+        D = (Wc - Lc).double()
+        r0 = torch.from_numpy(m["range0"]).to(device)
+        r1 = torch.from_numpy(m["range1"]).to(device)
+        out[i, :1326] = (0.5 * (D @ r1)).cpu().numpy()
+        out[i, 1326:] = (0.5 * (D @ r0)).cpu().numpy()
+    return out

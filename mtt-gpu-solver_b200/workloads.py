@@ -9,6 +9,8 @@ drawn from numpy's PCG64 generator with a fixed seed.
 * river_batch (config 2): n uneven river subgames; per subgame 1-4 bet sizes
   from U[25%, 200%], raise cap 1-3, supports of 200-1,081 combos with
   lognormal(0, 1) weights, pot U[20, 200], SPR U[0.5, 12].
+* diff_boards (config 3): n seeded river boards with the config-0 tree and
+  uniform ranges, plus N(0, 1) strategy logits per node and hand.
 """
 import numpy as np
 
@@ -67,3 +69,51 @@ def river_batch(n=4096, seed=2, min_support=200, max_support=1081, max_sizes=4):
             g[f"range{p}"] = w
         subs.append(g)
     return subs
+
+
+def diff_boards(n=1024, seed=3, n_hands=None):
+    """Config 3 (differentiable EV): n river subgames with config-0 trees
+    (pot 100, stack 200, bets {50%, 100%} + all-in, one raise) on boards drawn
+    from the seed, uniform ranges over the board's live combos (or n_hands of
+    them), and logits [rows_p][H_p] drawn N(0, 1) per node and hand."""
+    rng = np.random.default_rng(seed)
+    nodes, rows, _ = build_tree(100.0, 200.0, [0.5, 1.0], raise_cap=1)
+    subs, logits = [], []
+    for _ in range(n):
+        board = draw_board(rng)
+        live = live_combos(board)
+        if n_hands is not None:
+            live = np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
+        r = np.full(len(live), 1.0 / len(live), dtype=np.float32)
+        subs.append({"nodes": nodes, "rows": rows, "board": board, "combos0": live, "combos1": live.copy(),
+                     "range0": r, "range1": r.copy(), "pot": 100.0})
+        logits.append((rng.standard_normal((int(rows[0]), len(live))).astype(np.float32),
+                       rng.standard_normal((int(rows[1]), len(live))).astype(np.float32)))
+    return subs, logits
+
+
+def multiway_icm(seed=4, n_hands=None, pot_bb=4.0):
+    """Config 4 (four-player ICM river): eight seats with stacks drawn
+    lognormal(log 20 bb, 0.5); seats 0-3 are in the hand; payouts 50/30/20;
+    Malmuth-Harville bubble factors (FP64, host); a seeded river board;
+    Dirichlet(0.3) ranges over the 1,326 combos with board-blocked combos
+    removed (the live combos, or n_hands of them); the tree has bets {50%,
+    100%} and one pot-sized raise (677 nodes at these depths), pot_bb of dead
+    money."""
+    from . import multiway as mw
+    rng = np.random.default_rng(seed)
+    stacks = rng.lognormal(np.log(20.0), 0.5, size=8)
+    payouts = [0.5, 0.3, 0.2]
+    bf = mw.bubble_factors(stacks, payouts, [0, 1, 2, 3])
+    board = draw_board(rng)
+    live = live_combos(board)
+    if n_hands is not None:
+        live = np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
+    behind = [float(np.round(s - pot_bb / 4, 3)) for s in stacks[:4]]
+    nodes, rows, _ = mw.build_tree(pot_bb, behind, [0.5, 1.0], 1.0, 1)
+    ranges = []
+    for _ in range(4):
+        w = rng.dirichlet(np.full(1326, 0.3))[live.astype(np.int64)]
+        ranges.append((w / w.sum()).astype(np.float32))
+    return {"nodes": nodes, "rows": rows, "board": board, "combos": live, "ranges": ranges, "bubble": bf,
+            "pot": pot_bb, "stacks": stacks, "payouts": payouts}

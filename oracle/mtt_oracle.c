@@ -528,7 +528,7 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
  * (behaviour probabilities), plus best-response values. */
 static int orc_values_fp64(const orc_game* g, const double* pol0, const double* pol1,
                            double* br_root0, double* br_root1,
-                           double* ev_root0, double* ev_root1, double* Z) {
+                           double* ev_root0, double* ev_root1, double* Z, const double* const* rng) {
     orc_ctx c;
     int st = orc_ctx_init(&c, g);
     if (st) return st;
@@ -539,7 +539,7 @@ static int orc_values_fp64(const orc_game* g, const double* pol0, const double* 
         reach[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
         br[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
         ev[p] = (double*)calloc((size_t)n * (size_t)H[p] + 1, sizeof(double));
-        for (int h = 0; h < H[p]; ++h) reach[p][h] = g->range[p][h];
+        for (int h = 0; h < H[p]; ++h) reach[p][h] = rng ? rng[p][h] : (double)g->range[p][h];
     }
     int Hmax = H[0] > H[1] ? H[0] : H[1];
     double* tv = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
@@ -618,8 +618,9 @@ static int orc_values_fp64(const orc_game* g, const double* pol0, const double* 
     double z = 0.0;
     for (int h = 0; h < H[0]; ++h) {
         double m = 0.0;
-        for (int j = 0; j < H[1]; ++j) if (!(c.hmask[0][h] & c.hmask[1][j])) m += g->range[1][j];
-        z += (double)g->range[0][h] * m;
+        for (int j = 0; j < H[1]; ++j)
+            if (!(c.hmask[0][h] & c.hmask[1][j])) m += rng ? rng[1][j] : (double)g->range[1][j];
+        z += (rng ? rng[0][h] : (double)g->range[0][h]) * m;
     }
     *Z = z;
     if (br_root0) memcpy(br_root0, br[0], sizeof(double) * (size_t)H[0]);
@@ -658,7 +659,7 @@ int orc_best_response(const orc_game* g, const float* S0, const float* S1, doubl
     double* e0 = (double*)malloc(sizeof(double) * (size_t)(H0 + 1));
     double* e1 = (double*)malloc(sizeof(double) * (size_t)(H1 + 1));
     double Z = 0.0;
-    int st = orc_values_fp64(g, pol0, pol1, b0, b1, e0, e1, &Z);
+    int st = orc_values_fp64(g, pol0, pol1, b0, b1, e0, e1, &Z, NULL);
     if (st == MTT_OK) {
         double br0 = 0, br1 = 0, ev0 = 0, ev1 = 0;
         for (int h = 0; h < H0; ++h) { br0 += g->range[0][h] * b0[h]; ev0 += g->range[0][h] * e0[h]; }
@@ -679,7 +680,7 @@ int orc_strategy_values(const orc_game* g, const float* sigma0, const float* sig
     for (size_t k = 0; k < (size_t)rows0 * (size_t)g->H[0]; ++k) pol0[k] = sigma0[k];
     for (size_t k = 0; k < (size_t)rows1 * (size_t)g->H[1]; ++k) pol1[k] = sigma1[k];
     double Z = 0.0;
-    int st = orc_values_fp64(g, pol0, pol1, NULL, NULL, out_cfv0, out_cfv1, &Z);
+    int st = orc_values_fp64(g, pol0, pol1, NULL, NULL, out_cfv0, out_cfv1, &Z, NULL);
     if (st == MTT_OK && ev_out) {
         double ev = 0.0;
         for (int h = 0; h < g->H[0]; ++h) ev += (double)g->range[0][h] * out_cfv0[h];
@@ -687,4 +688,281 @@ int orc_strategy_values(const orc_game* g, const float* sigma0, const float* sig
     }
     free(pol0); free(pol1);
     return st;
+}
+
+/* Differentiable-EV oracle: both players play softmax(logits) per node and
+ * hand; FP64 throughout.  EV0 = sum over hands of range0 * cfv0(root) in
+ * chips (the values of orc_values_fp64, i.e. kernel_evaluate_terminals and
+ * kernel_backward_sweep of honest_multistreet_solver.cu:128-249 with card
+ * removal). */
+int orc_softmax_ev(const orc_game* g, const double* logits0, const double* logits1,
+                   const double* range0, const double* range1, double* ev0, double* cfv0, double* cfv1) {
+    const double* lg[2] = {logits0, logits1};
+    double* pol[2];
+    for (int p = 0; p < 2; ++p) {
+        const int H = g->H[p];
+        pol[p] = (double*)calloc((size_t)g->rows[p] * (size_t)H + 1, sizeof(double));
+        for (int i = 0; i < g->n_nodes; ++i) {
+            const mtt_node* nd = &g->nodes[i];
+            if (nd->type != MTT_NODE_DECISION || nd->player != p) continue;
+            const int A = nd->num_actions, r0 = nd->infoset_offset;
+            for (int h = 0; h < H; ++h) {
+                double m = -1e300, den = 0.0;
+                for (int a = 0; a < A; ++a) { double l = lg[p][(size_t)(r0 + a) * H + h]; if (l > m) m = l; }
+                for (int a = 0; a < A; ++a) den += exp(lg[p][(size_t)(r0 + a) * H + h] - m);
+                for (int a = 0; a < A; ++a)
+                    pol[p][(size_t)(r0 + a) * H + h] = exp(lg[p][(size_t)(r0 + a) * H + h] - m) / den;
+            }
+        }
+    }
+    const double* rng[2] = {range0, range1};
+    double* c0 = (double*)malloc(sizeof(double) * ((size_t)g->H[0] + 1));
+    double* c1 = (double*)malloc(sizeof(double) * ((size_t)g->H[1] + 1));
+    double Z = 0.0;
+    int st = orc_values_fp64(g, pol[0], pol[1], NULL, NULL, c0, c1, &Z, rng);
+    if (st == MTT_OK) {
+        double ev = 0.0;
+        for (int h = 0; h < g->H[0]; ++h) ev += range0[h] * c0[h];
+        if (ev0) *ev0 = ev;
+        if (cfv0) memcpy(cfv0, c0, sizeof(double) * (size_t)g->H[0]);
+        if (cfv1) memcpy(cfv1, c1, sizeof(double) * (size_t)g->H[1]);
+    }
+    free(c0); free(c1); free(pol[0]); free(pol[1]);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Four-player river CFR: restates kernel_4way_forward_sweep,               */
+/* kernel_4way_evaluate_terminals and kernel_4way_backward_cfr_plus          */
+/* (src/postflop/multiway_4way_engine.cu:41-257) with simultaneous updates;  */
+/* FP32 storage, terminal values in FP64 rounded to float.                   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int H, n;
+    int* pos; int* gs; int* ge;      /* rank position, rank-group bounds per hand */
+} orc_mw_ctx;
+
+static void orc_mw_ranks(const orc_mw_game* g, orc_mw_ctx* c) {
+    int H = g->H;
+    uint32_t* sc = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(H + 1));
+    int* ord = (int*)malloc(sizeof(int) * (size_t)(H + 1));
+    for (int h = 0; h < H; ++h) {
+        uint8_t cards[7] = {g->board[0], g->board[1], g->board[2], g->board[3], g->board[4],
+                            g->cards[2 * h], g->cards[2 * h + 1]};
+        sc[h] = orc_score7(cards);
+        ord[h] = h;
+    }
+    /* stable insertion sort by score (ties keep index order) */
+    for (int i = 1; i < H; ++i) {
+        int x = ord[i], j = i - 1;
+        while (j >= 0 && sc[ord[j]] > sc[x]) { ord[j + 1] = ord[j]; --j; }
+        ord[j + 1] = x;
+    }
+    c->pos = (int*)malloc(sizeof(int) * (size_t)(H + 1));
+    c->gs = (int*)malloc(sizeof(int) * (size_t)(H + 1));
+    c->ge = (int*)malloc(sizeof(int) * (size_t)(H + 1));
+    for (int i = 0; i < H;) {
+        int j = i;
+        while (j < H && sc[ord[j]] == sc[ord[i]]) ++j;
+        for (int k = i; k < j; ++k) { c->pos[ord[k]] = k; c->gs[ord[k]] = i; c->ge[ord[k]] = j; }
+        i = j;
+    }
+    c->H = H;
+    free(sc); free(ord);
+}
+
+/* Terminal values of all four players at node i (kernel_4way_evaluate_terminals). */
+static void orc_mw_terminal(const orc_mw_game* g, const orc_mw_ctx* c, int i, int sem,
+                            const float* const* reach /* [4] at node i */, float* out /* [4][H] */) {
+    const mtt_mw_node* nd = &g->nodes[i];
+    int H = g->H;
+    double tot[4];
+    double* cdf[4];
+    for (int o = 0; o < 4; ++o) {
+        cdf[o] = (double*)calloc((size_t)H + 1, sizeof(double));
+        double* byp = (double*)calloc((size_t)H + 1, sizeof(double));
+        for (int h = 0; h < H; ++h) byp[c->pos[h]] = reach[o][h];
+        double run = 0.0;
+        for (int k = 0; k < H; ++k) { cdf[o][k] = run; run += byp[k]; }
+        cdf[o][H] = run;
+        tot[o] = run;
+        free(byp);
+    }
+    int am = nd->active_mask;
+    for (int p = 0; p < 4; ++p) {
+        double others = 1.0;
+        for (int o = 0; o < 4; ++o) if (o != p) others *= tot[o];
+        for (int h = 0; h < H; ++h) {
+            double v;
+            if (nd->type == MTT_NODE_FOLD) {
+                int w = 0;
+                while (!((am >> w) & 1)) ++w;
+                v = (p == w ? (double)nd->pot_size - (double)nd->committed[p]
+                            : -(double)g->bubble[p * 4 + w] * (double)nd->committed[p]) * others;
+            } else if (!((am >> p) & 1)) {
+                v = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p] * others;
+            } else {
+                double gain = (double)nd->pot_size - (double)nd->committed[p];
+                double loss = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p];
+                double inact = 1.0, PW = 1.0;
+                int opp[3], no = 0;
+                for (int o = 0; o < 4; ++o) {
+                    if (o == p) continue;
+                    if ((am >> o) & 1) { PW *= tot[o]; opp[no++] = o; } else inact *= tot[o];
+                }
+                if (sem == ORC_SEM_REFERENCE) {
+                    double F = 1.0;
+                    for (int k = 0; k < no; ++k) F *= cdf[opp[k]][c->pos[h]];
+                    v = (gain * F + loss * (PW - F)) * inact;
+                } else {
+                    double L[3], E[3], LE = 1.0, share = 0.0;
+                    for (int k = 0; k < no; ++k) {
+                        L[k] = cdf[opp[k]][c->gs[h]];
+                        E[k] = cdf[opp[k]][c->ge[h]] - L[k];
+                        LE *= L[k] + E[k];
+                    }
+                    for (int T = 0; T < (1 << no); ++T) {
+                        double pr = 1.0;
+                        int nt = 0;
+                        for (int k = 0; k < no; ++k) {
+                            if ((T >> k) & 1) { pr *= E[k]; ++nt; } else pr *= L[k];
+                        }
+                        share += pr * ((double)nd->pot_size / (1 + nt) - (double)nd->committed[p]);
+                    }
+                    v = (share + loss * (PW - LE)) * inact;
+                }
+            }
+            out[(size_t)p * H + h] = (float)v;
+        }
+    }
+    for (int o = 0; o < 4; ++o) free(cdf[o]);
+}
+
+static float orc_mw_sigma(const float* B, int H, int A, int k, int h, int avg) {
+    float sum = 0.0f;
+    for (int j = 0; j < A; ++j) sum += avg ? B[(size_t)j * H + h] : fmaxf(B[(size_t)j * H + h], 0.0f);
+    float invA = 1.0f / (float)A;
+    if (avg) return sum > 0.0f ? B[(size_t)k * H + h] / sum : invA;
+    return sum > 1e-7f ? fmaxf(B[(size_t)k * H + h], 0.0f) / sum : invA;
+}
+
+/* One sweep: reach down, terminals, values up; updates when upd != 0. */
+static void orc_mw_sweep(const orc_mw_game* g, const orc_mw_ctx* c, const orc_cfr_params* prm, int t,
+                         float** R, float** S, float* reach, float* cfv, int upd, int sem) {
+    int n = g->n_nodes, H = g->H;
+    size_t HS = (size_t)4 * H;
+    for (int p = 0; p < 4; ++p) for (int h = 0; h < H; ++h) reach[(size_t)p * H + h] = g->range[p][h];
+    for (int i = 0; i < n; ++i) {
+        const mtt_mw_node* nd = &g->nodes[i];
+        if (nd->type != MTT_NODE_DECISION) continue;
+        int p = nd->player, A = nd->num_actions;
+        const float* B = (upd ? R[p] : S[p]) + (size_t)nd->infoset_offset * H;
+        for (int a = 0; a < A; ++a) {
+            int ch = nd->children_offset + a;
+            memcpy(&reach[(size_t)ch * HS], &reach[(size_t)i * HS], sizeof(float) * HS);
+            for (int h = 0; h < H; ++h)
+                reach[(size_t)ch * HS + (size_t)p * H + h] = reach[(size_t)i * HS + (size_t)p * H + h] *
+                                                             orc_mw_sigma(B, H, A, a, h, !upd);
+        }
+    }
+    double tm1 = (double)(t - 1);
+    float w_lin = (float)pow((double)t, (double)prm->avg_power);
+    float dpos = (float)(pow(tm1, (double)prm->alpha) / (pow(tm1, (double)prm->alpha) + 1.0));
+    float dneg = (float)(pow(tm1, (double)prm->beta) / (pow(tm1, (double)prm->beta) + 1.0));
+    float dstr = (float)pow(tm1 / (double)t, (double)prm->gamma);
+    for (int i = n - 1; i >= 0; --i) {
+        const mtt_mw_node* nd = &g->nodes[i];
+        float* out = &cfv[(size_t)i * HS];
+        if (nd->type != MTT_NODE_DECISION) {
+            const float* rp[4];
+            for (int p = 0; p < 4; ++p) rp[p] = &reach[(size_t)i * HS + (size_t)p * H];
+            orc_mw_terminal(g, c, i, sem, rp, out);
+            continue;
+        }
+        int p = nd->player, A = nd->num_actions;
+        for (int q = 0; q < 4; ++q) {
+            for (int h = 0; h < H; ++h) {
+                if (q != p) {
+                    float s = 0.0f;
+                    for (int a = 0; a < A; ++a) s += cfv[(size_t)(nd->children_offset + a) * HS + (size_t)q * H + h];
+                    out[(size_t)q * H + h] = s;
+                }
+            }
+        }
+        float* Rb = R[p] + (size_t)nd->infoset_offset * H;
+        float* Sb = S[p] + (size_t)nd->infoset_offset * H;
+        const float* B = upd ? Rb : Sb;
+        for (int h = 0; h < H; ++h) {
+            float sg[MTT_MW_MAX_ACTIONS], v = 0.0f;
+            for (int a = 0; a < A; ++a) {
+                sg[a] = orc_mw_sigma(B, H, A, a, h, !upd);
+                v = fmaf(sg[a], cfv[(size_t)(nd->children_offset + a) * HS + (size_t)p * H + h], v);
+            }
+            out[(size_t)p * H + h] = v;
+            if (!upd) continue;
+            float r = reach[(size_t)i * HS + (size_t)p * H + h];
+            float wr = r * w_lin;
+            for (int a = 0; a < A; ++a) {
+                float qk = cfv[(size_t)(nd->children_offset + a) * HS + (size_t)p * H + h];
+                float rk = Rb[(size_t)a * H + h], inst = qk - v;
+                float sv = Sb[(size_t)a * H + h];
+                if (prm->algo == ORC_ALGO_DCFR) {
+                    Rb[(size_t)a * H + h] = rk * (rk > 0.0f ? dpos : dneg) + inst;
+                    Sb[(size_t)a * H + h] = fmaf(r, sg[a], sv * dstr);
+                } else {
+                    Rb[(size_t)a * H + h] = fmaxf(0.0f, rk + inst);
+                    Sb[(size_t)a * H + h] = fmaf(wr, sg[a], sv);
+                }
+            }
+        }
+    }
+}
+
+int orc_mw_solve(const orc_mw_game* g, const orc_cfr_params* prm, float* R[4], float* S[4], float* root_cfv,
+                 double* values) {
+    if (!g || !prm || g->H < 1) return MTT_ERR_INVALID;
+    orc_mw_ctx c;
+    orc_mw_ranks(g, &c);
+    int n = g->n_nodes, H = g->H;
+    size_t HS = (size_t)4 * H;
+    float* reach = (float*)calloc((size_t)n * HS + 1, sizeof(float));
+    float* cfv = (float*)calloc((size_t)n * HS + 1, sizeof(float));
+    for (int p = 0; p < 4; ++p) {
+        memset(R[p], 0, sizeof(float) * (size_t)g->rows[p] * (size_t)H);
+        memset(S[p], 0, sizeof(float) * (size_t)g->rows[p] * (size_t)H);
+    }
+    for (int t = 1; t <= prm->iters; ++t) orc_mw_sweep(g, &c, prm, t, R, S, reach, cfv, 1, prm->semantics);
+    if (root_cfv) memcpy(root_cfv, cfv, sizeof(float) * HS);
+    if (values) {
+        orc_mw_sweep(g, &c, prm, 1, R, S, reach, cfv, 0, prm->semantics);
+        for (int p = 0; p < 4; ++p) {
+            double acc = 0.0;
+            for (int h = 0; h < H; ++h) acc += (double)g->range[p][h] * (double)cfv[(size_t)p * H + h];
+            values[p] = acc;
+        }
+    }
+    free(reach); free(cfv); free(c.pos); free(c.gs); free(c.ge);
+    return MTT_OK;
+}
+
+/* Malmuth-Harville equity by direct enumeration of the ordered finishers of
+ * the paid places (an independent restatement of the subset recursion). */
+static void orc_icm_rec(const double* st, int n, const double* pay, int m, int depth, unsigned used, double rest,
+                        double prob, double* out) {
+    if (depth == m || !(rest > 0.0)) return;
+    for (int i = 0; i < n; ++i) {
+        if ((used >> i) & 1u) continue;
+        double p = prob * st[i] / rest;
+        if (p == 0.0) continue;
+        out[i] += p * pay[depth];
+        orc_icm_rec(st, n, pay, m, depth + 1, used | (1u << i), rest - st[i], p, out);
+    }
+}
+
+int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, double* out) {
+    if (n < 1 || n > 16 || m < 0 || m > n) return MTT_ERR_INVALID;
+    double S = 0.0;
+    for (int i = 0; i < n; ++i) { out[i] = 0.0; S += stacks[i]; }
+    orc_icm_rec(stacks, n, payouts, m, 0, 0u, S, 1.0, out);
+    return MTT_OK;
 }

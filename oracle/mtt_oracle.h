@@ -90,6 +90,33 @@ int orc_best_response(const orc_game* g, const float* S0, const float* S1, doubl
 int orc_strategy_values(const orc_game* g, const float* sigma0, const float* sigma1,
                         double* out_cfv0, double* out_cfv1, double* ev_out);
 
+/* EV of P0 in chips when both players play softmax(logits_p) ([rows_p][H_p],
+ * per node and hand) with root ranges range_p (FP64 throughout); cfv_p
+ * (optional): root counterfactual values [H_p]. */
+int orc_softmax_ev(const orc_game* g, const double* logits0, const double* logits1,
+                   const double* range0, const double* range1, double* ev0, double* cfv0, double* cfv1);
+
+/* --- four-player river CFR: multiway_4way_engine.cu:41-257 ---------------- */
+typedef struct orc_mw_game {
+    const mtt_mw_node* nodes;
+    int32_t n_nodes;
+    int32_t rows[4];
+    const uint8_t* board;      /* 5 cards */
+    int32_t H;                 /* one combo axis shared by the four players */
+    const uint8_t* cards;      /* H x 2 hole cards */
+    const float* range[4];
+    float bubble[16];
+} orc_mw_game;
+
+/* prm: iters, algo (+alpha/beta/gamma), semantics, avg_power (alternate is
+ * ignored: the four players update simultaneously).  R[p], S[p]: [rows_p][H];
+ * root_cfv (optional): [4][H] of the last iteration; values (optional, [4]):
+ * each player's range EV (chips) under the average strategies. */
+int orc_mw_solve(const orc_mw_game* g, const orc_cfr_params* prm, float* R[4], float* S[4], float* root_cfv,
+                 double* values);
+/* Malmuth-Harville equity by enumerating the ordered finishers of the m paid places. */
+int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,7 @@ def lib():
         L.orc_cfr_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]; L.orc_cfr_solve.restype = ctypes.c_int
         L.orc_best_response.argtypes = [vp, vp, vp, vp]; L.orc_best_response.restype = ctypes.c_int
         L.orc_strategy_values.argtypes = [vp, vp, vp, vp, vp, vp]; L.orc_strategy_values.restype = ctypes.c_int
+        L.orc_softmax_ev.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]; L.orc_softmax_ev.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -163,3 +164,78 @@ def strategy_values(sub, sigma0, sigma1):
     if st:
         raise RuntimeError(f"orc_strategy_values status {st}")
     return c0, c1, ev.value
+
+
+def softmax_ev(sub, logits0, logits1, range0=None, range1=None):
+    """EV0 (chips) and root CFVs when both players play softmax(logits_p)
+    ([rows_p][H_p] float64), FP64 throughout."""
+    gh = _GameHolder(sub)
+    l0 = np.ascontiguousarray(logits0, np.float64); l1 = np.ascontiguousarray(logits1, np.float64)
+    r0 = np.ascontiguousarray(sub["range0"] if range0 is None else range0, np.float64)
+    r1 = np.ascontiguousarray(sub["range1"] if range1 is None else range1, np.float64)
+    c0 = np.zeros(gh.H[0], np.float64); c1 = np.zeros(gh.H[1], np.float64)
+    ev = ctypes.c_double()
+    st = lib().orc_softmax_ev(ctypes.byref(gh.g), l0.ctypes.data, l1.ctypes.data, r0.ctypes.data, r1.ctypes.data,
+                              ctypes.byref(ev), c0.ctypes.data, c1.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_softmax_ev status {st}")
+    return ev.value, c0, c1
+
+
+vp = ctypes.c_void_p
+
+
+class MwGame(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int32), ("rows", ctypes.c_int32 * 4),
+                ("board", ctypes.c_void_p), ("H", ctypes.c_int32), ("cards", ctypes.c_void_p),
+                ("range", ctypes.c_void_p * 4), ("bubble", ctypes.c_float * 16)]
+
+
+def mw_solve(sub, iters, algo=0, alpha=1.5, beta=0.0, gamma=2.0, semantics=0, avg_power=1.0):
+    """Four-player oracle: dict with R, S (lists of [rows_p][H]), cfv [4][H], values [4]."""
+    L = lib()
+    if not getattr(L, "_mw_sig", False):
+        L.orc_mw_solve.argtypes = [vp, vp, vp, vp, vp, vp]; L.orc_mw_solve.restype = ctypes.c_int
+        L.orc_icm_equity.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]; L.orc_icm_equity.restype = ctypes.c_int
+        L._mw_sig = True
+    nodes = np.ascontiguousarray(sub["nodes"])
+    board = np.ascontiguousarray(np.asarray(sub["board"], np.uint8))
+    cards = np.ascontiguousarray(_combo_cards(sub["combos"]))
+    rg = [np.ascontiguousarray(r, np.float32) for r in sub["ranges"]]
+    g = MwGame()
+    g.nodes = nodes.ctypes.data
+    g.n_nodes = len(nodes)
+    for p in range(4):
+        g.rows[p] = int(sub["rows"][p])
+        g.range[p] = rg[p].ctypes.data
+    g.board = board.ctypes.data
+    g.H = len(cards)
+    g.cards = cards.ctypes.data
+    bf = np.ones(16) if sub.get("bubble") is None else np.asarray(sub["bubble"], np.float64).reshape(16)
+    for k in range(16):
+        g.bubble[k] = float(bf[k])
+    H = len(cards)
+    R = [np.zeros((int(sub["rows"][p]), H), np.float32) for p in range(4)]
+    S = [np.zeros((int(sub["rows"][p]), H), np.float32) for p in range(4)]
+    cfv = np.zeros((4, H), np.float32)
+    vals = np.zeros(4, np.float64)
+    pr = (ctypes.c_void_p * 4)(*[R[p].ctypes.data for p in range(4)])
+    ps = (ctypes.c_void_p * 4)(*[S[p].ctypes.data for p in range(4)])
+    prm = CfrParams(int(iters), int(algo), float(alpha), float(beta), float(gamma), int(semantics), 0,
+                    float(avg_power))
+    st = L.orc_mw_solve(ctypes.byref(g), ctypes.byref(prm), pr, ps, cfv.ctypes.data, vals.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_mw_solve status {st}")
+    return {"R": R, "S": S, "cfv": cfv, "values": vals}
+
+
+def icm_equity(stacks, payouts):
+    L = lib()
+    L.orc_icm_equity.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
+    L.orc_icm_equity.restype = ctypes.c_int
+    st = np.ascontiguousarray(stacks, np.float64)
+    pay = np.ascontiguousarray(payouts, np.float64)
+    out = np.zeros(len(st), np.float64)
+    if L.orc_icm_equity(st.ctypes.data, len(st), pay.ctypes.data, len(pay), out.ctypes.data):
+        raise RuntimeError("orc_icm_equity failed")
+    return out

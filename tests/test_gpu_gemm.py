@@ -1,0 +1,66 @@
+"""tcgen05 BF16 GEMM against a plain PyTorch fp32 reference of the same op
+(fp32 matmul of the same bf16 values).  Tolerance (written here): fp32 output
+within 1e-5 * sqrt(K) * max|C| + 1e-6 (summation order only); bf16 output
+within one bf16 ulp (2^-8 relative) of the rounded reference."""
+import math
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref(A, B, bias, relu, mask):
+    C = A.float() @ B.float().T
+    if bias is not None:
+        C = C + bias
+    if relu:
+        C = C.clamp_min(0)
+    if mask is not None:
+        C = C * (mask.float() > 0)
+    return C
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (200, 130, 72), (1000, 2652, 1024),
+                                   (512, 1024, 2752), (7, 9, 8)])
+def test_gemm_fp32_out(mtt, cuda, M, N, K):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(M * 31 + N)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).to(cuda)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).to(cuda)
+    C = mtt.gemm_bf16(A, B)
+    R = _ref(A, B, None, False, None)
+    tol = 1e-5 * math.sqrt(K) * float(R.abs().max()) + 1e-6
+    assert float((C - R).abs().max()) <= tol
+
+
+def test_gemm_bias_relu_bf16_and_mask(mtt, cuda):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(5)
+    M, N, K = 384, 256, 512
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).to(cuda)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).to(cuda)
+    bias = torch.randn(N, generator=g).to(cuda)
+    C = mtt.gemm_bf16(A, B, bias=bias, relu=True, out_bf16=True)
+    R = _ref(A, B, bias, True, None)
+    assert C.dtype == torch.bfloat16
+    assert float(((C.float() - R).abs() / (R.abs() + 1e-3)).max()) <= 2 ** -8 + 1e-6
+    mask = torch.randn(M, N, generator=g).to(torch.bfloat16).to(cuda)
+    C2 = mtt.gemm_bf16(A, B, mask=mask)
+    R2 = _ref(A, B, None, False, mask)
+    assert float((C2 - R2).abs().max()) <= 1e-5 * math.sqrt(K) * float(R2.abs().max()) + 1e-6
+    assert bool((C2[mask.float() <= 0] == 0).all())
+
+
+def test_gemm_strided_operands(mtt, cuda):
+    """Row strides larger than K (views into wider buffers) and an output
+    written into a wider matrix."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(9)
+    Abig = torch.randn(300, 200, generator=g).to(torch.bfloat16).to(cuda)
+    Bbig = torch.randn(140, 136, generator=g).to(torch.bfloat16).to(cuda)
+    A, B = Abig[:, :128], Bbig[:, :128]
+    out = torch.zeros(300, 160, device=cuda)
+    mtt.gemm_bf16(A, B, out=out[:, :140])
+    R = _ref(A, B, None, False, None)
+    assert float((out[:, :140] - R).abs().max()) <= 1e-5 * math.sqrt(128) * float(R.abs().max()) + 1e-6
+    assert float(out[:, 140:].abs().max()) == 0.0
