@@ -337,6 +337,42 @@ int mtt_leafnet_params(mtt_leafnet* n, int32_t layer, float* h_w, float* h_b, fl
 int mtt_leafnet_check(mtt_leafnet* n);
 int mtt_leafnet_destroy(mtt_leafnet* n);
 
+/* ------------------------------------------------- preflop anchor chain */
+#define MTT_PF_REFERENCE 0   /* the reference's arithmetic, quirks included (see preflop.cu) */
+#define MTT_PF_CORRECT   1   /* valid class cards, sampling without replacement, every
+                                flop-compatible combo, ties count one half */
+/* 169 x 169 all-in equities of the hand classes, d_out[h*169 + v]
+ * (kernel_gen_preflop_matrix, src/preflop/preflop_grid_generator.cu:95-127:
+ * 3,000 LCG board samples per pair); d_wins / d_ties (optional, together)
+ * receive the integer counts. */
+int mtt_pf_allin_matrix(int32_t mode, float* d_out, int32_t* d_wins, int32_t* d_ties, void* stream);
+/* Class-reduced flop equity matrices of n flops (3 cards each):
+ * d_out[f][v][h] (kernel_gen_100_flop_matrices + kernel_reduce_combo_to_class_matrices,
+ * preflop_grid_generator.cu:130-223), without the 1,216 x 1,216 combo
+ * matrices of every flop resident at once. */
+int mtt_pf_flop_class_matrices(int32_t mode, const uint8_t* d_flops, int32_t n, float* d_out, void* stream);
+typedef struct mtt_pf_params {
+    int32_t iters;       /* 500 in the reference */
+    float   stack_bb;    /* 20 */
+    float   bubble;      /* 1.35 */
+    float   dead_pot;    /* 2.5 */
+} mtt_pf_params;
+/* DCFR over the closed BTN-vs-BB preflop tree (kernel_cosolve_100_board_matrices,
+ * kernel_build_closed_preflop_cfvs, kernel_dcfr_step, kernel_update_dynamic_reaches
+ * and the loop at preflop_grid_generator.cu:228-421,588-614).  d_sums / d_sigma
+ * ([10][192]): strategy sums / last strategies of the nodes BTN root (fold,
+ * min-raise, jam), BB vs min-raise (fold, call, 3-bet jam), BTN vs 3-bet (fold,
+ * call), BB vs open jam (fold, call), one 192-wide row per action. */
+int mtt_pf_dcfr(const float* d_flop_weights, const float* d_class_mats, int32_t n_flops, const float* d_allin,
+                const mtt_pf_params* p, float* d_sums, float* d_sigma, void* stream);
+/* Read a flop-subset file (uint32 count, then per flop c1, c2, c3, pad, float
+ * weight; preflop_grid_generator.cu:446-459).  path NULL: data/mtt_subset.bin,
+ * then ./mtt_subset.bin.  h_flops NULL: only *n.  Host only. */
+int mtt_pf_read_subset(const char* path, uint8_t* h_flops, float* h_weights, int32_t capacity, int32_t* n);
+/* Class (0..168) of the combo c1 < c2 as the reference numbers them (pairs AA..22,
+ * suited, offsuit); -1 if invalid. */
+int mtt_pf_combo_class(int32_t c1, int32_t c2);
+
 /* ------------------------------------------- ICM (Malmuth-Harville, FP64) */
 /* Tournament equity of n seats with chip stacks[n] and m payouts[m] (prize
  * for 1st, 2nd, ...): the probability that seat i finishes k-th is the

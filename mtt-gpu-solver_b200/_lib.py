@@ -67,6 +67,11 @@ class MwSubgame(ctypes.Structure):
                 ("ranges", ctypes.c_void_p * 4), ("bubble", ctypes.c_float * 16)]
 
 
+class PfParams(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("stack_bb", ctypes.c_float), ("bubble", ctypes.c_float),
+                ("dead_pot", ctypes.c_float)]
+
+
 class MttError(RuntimeError):
     def __init__(self, fn, status, cuda_err=0):
         super().__init__(f"{fn} failed: {STATUS.get(status, status)} (status {status}, cudaError {cuda_err})")
@@ -119,6 +124,11 @@ def lib():
         "mtt_leafnet_params": ([vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_leafnet_check": ([vp], ctypes.c_int),
         "mtt_leafnet_destroy": ([vp], ctypes.c_int),
+        "mtt_pf_allin_matrix": ([i32, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_pf_flop_class_matrices": ([i32, vp, i32, vp, vp], ctypes.c_int),
+        "mtt_pf_dcfr": ([vp, vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
+        "mtt_pf_read_subset": ([ctypes.c_char_p, vp, vp, i32, vp], ctypes.c_int),
+        "mtt_pf_combo_class": ([i32, i32], ctypes.c_int),
         "mtt_icm_equity": ([vp, i32, vp, i32, vp], ctypes.c_int),
         "mtt_icm_bubble_factors": ([vp, i32, vp, i32, vp, i32, vp], ctypes.c_int),
         "mtt_mw_tree_build": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),

@@ -376,51 +376,6 @@ __device__ __forceinline__ void bwd_sum_fixed(const float4* __restrict__ qc, flo
     out[g] = so;
 }
 
-template <int A>
-__device__ __forceinline__ void bwd_update_fixed(float4* __restrict__ Rb, float4* __restrict__ Sb,
-                                                 const float4* __restrict__ qc, const float4* __restrict__ rr,
-                                                 float4* __restrict__ out, int H4, int HS4, int g, bool ds, bool dcfr,
-                                                 float4 tb) {
-    float4 rk[A], qk[A];
-#pragma unroll
-    for (int k = 0; k < A; ++k) { rk[k] = Rb[(size_t)k * H4 + g]; qk[k] = qc[(size_t)k * HS4 + g]; }
-    const float invA = __fdiv_rn(1.0f, (float)A);
-    float4 sum = f4(0.f);
-#pragma unroll
-    for (int k = 0; k < A; ++k) sum = add4(sum, max04(rk[k]));
-    float4 v = f4(0.f);
-#pragma unroll
-    for (int k = 0; k < A; ++k) v = fma4(rm4(max04(rk[k]), sum, invA), qk[k], v);
-    out[g] = v;
-    if (ds) {
-        const float4 r = rr[g];
-        const float4 wr = mul4(r, f4(tb.x));
-#pragma unroll
-        for (int k = 0; k < A; ++k) {
-            const float4 sg = rm4(max04(rk[k]), sum, invA);
-            float4 sv = Sb[(size_t)k * H4 + g];
-            sv = dcfr ? fma4(r, sg, mul4(sv, f4(tb.w))) : fma4(wr, sg, sv);
-            Sb[(size_t)k * H4 + g] = sv;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < A; ++k) {
-        float4 nr;
-        if (dcfr) {
-            nr.x = dcfr1(rk[k].x, __fsub_rn(qk[k].x, v.x), tb.y, tb.z);
-            nr.y = dcfr1(rk[k].y, __fsub_rn(qk[k].y, v.y), tb.y, tb.z);
-            nr.z = dcfr1(rk[k].z, __fsub_rn(qk[k].z, v.z), tb.y, tb.z);
-            nr.w = dcfr1(rk[k].w, __fsub_rn(qk[k].w, v.w), tb.y, tb.z);
-        } else {
-            nr.x = cfrplus1(rk[k].x, __fsub_rn(qk[k].x, v.x));
-            nr.y = cfrplus1(rk[k].y, __fsub_rn(qk[k].y, v.y));
-            nr.z = cfrplus1(rk[k].z, __fsub_rn(qk[k].z, v.z));
-            nr.w = cfrplus1(rk[k].w, __fsub_rn(qk[k].w, v.w));
-        }
-        Rb[(size_t)k * H4 + g] = nr;
-    }
-}
-
 // Forward sweep of one level: regret matching, children's reach and/or
 // strategy sums (kernel_forward_sweep, honest_multistreet_solver.cu:88-126).
 __global__ void __launch_bounds__(256, 3) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
@@ -638,7 +593,7 @@ __global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __rest
 
 // Backward sweep of one level for the updated players: counterfactual values
 // and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
-__global__ void __launch_bounds__(256, 2) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+__global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
@@ -695,19 +650,6 @@ __global__ void __launch_bounds__(256, 2) k_bwd(SolveDev a, const BwdItem* __res
         dneg = tb.z;
         w_lin = tb.x;
         dstr = tb.w;
-    }
-    {
-        const float4 tb = make_float4(w_lin, dpos, dneg, dstr);
-        float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
-        const float4* rr = reinterpret_cast<const float4*>(a.arena + it.hc);
-        switch (A) {
-            case 2: bwd_update_fixed<2>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
-            case 3: bwd_update_fixed<3>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
-            case 4: bwd_update_fixed<4>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
-            case 5: bwd_update_fixed<5>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
-            case 6: bwd_update_fixed<6>(Rb, Sb, qc, rr, out, H4, HS4, g, ds, dcfr, tb); return;
-            default: break;
-        }
     }
     // Rows and child values are re-read (L1 hits) instead of held in registers.
     {

@@ -117,3 +117,23 @@ def multiway_icm(seed=4, n_hands=None, pot_bb=4.0):
         ranges.append((w / w.sum()).astype(np.float32))
     return {"nodes": nodes, "rows": rows, "board": board, "combos": live, "ranges": ranges, "bubble": bf,
             "pot": pot_bb, "stacks": stacks, "payouts": payouts}
+
+
+def turn_dcfr(seed=1, n_hands=None):
+    """Config 1 (heads-up turn + river DCFR): a 4-card turn board from the
+    seed, 48 river cards; each player's range is a 1,326-entry Dirichlet(0.3)
+    weight vector with board-blocked combos removed (or n_hands of the live
+    combos); pot 60, stack 470; bets {33%, 75%, 150%} + all-in, 2 raises,
+    on both streets."""
+    rng = np.random.default_rng(seed)
+    board = draw_board(rng, 4)
+    live = live_combos(board)
+    nodes, rows, _ = build_tree(60.0, 470.0, [0.33, 0.75, 1.5], raise_cap=2, street=4, board=board)
+    g = {"nodes": nodes, "rows": rows, "board": board, "pot": 60.0}
+    for p in (0, 1):
+        w = rng.dirichlet(np.full(1326, 0.3))
+        c = live if n_hands is None else np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
+        r = w[c.astype(np.int64)]
+        g[f"combos{p}"] = c.astype(np.uint16)
+        g[f"range{p}"] = (r / r.sum()).astype(np.float32)
+    return g

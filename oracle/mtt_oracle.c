@@ -966,3 +966,269 @@ int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, do
     orc_icm_rec(stacks, n, payouts, m, 0, 0u, S, 1.0, out);
     return MTT_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Preflop anchor chain: restates src/preflop/preflop_grid_generator.cu      */
+/* (kernels :95-421, host set-up and loop :426-614) in reference mode.       */
+/* ------------------------------------------------------------------------ */
+#define PF_CLASSES 169
+#define PF_PAD 192
+#define PF_ALIVE 1176
+#define PF_PADDED 1216
+
+/* class_to_cards (:79-92), including its boundary behaviour */
+static void orc_pf_class_to_cards(int cls, uint8_t* h1, uint8_t* h2) {
+    if (cls < 13) { int r = 12 - cls; *h1 = (uint8_t)(r * 4 + 0); *h2 = (uint8_t)(r * 4 + 1); }
+    else {
+        int base = cls < 91 ? 13 : 91, r1 = 12, r2;
+        while (base + (r1 - 1) <= cls) base += r1--;
+        r2 = r1 - 1 - (cls - base);
+        *h1 = (uint8_t)(r1 * 4 + 0);
+        *h2 = (uint8_t)(r2 * 4 + (cls < 91 ? 0 : 1));
+    }
+}
+
+/* combo -> class as the host set-up computes it (:475-483) */
+int orc_pf_combo_class(int c1, int c2) {
+    int r1 = c1 / 4, s1 = c1 % 4, r2 = c2 / 4, s2 = c2 % 4;
+    int hi = r1 > r2 ? r1 : r2, lo = r1 < r2 ? r1 : r2;
+    if (r1 == r2) return 12 - hi;
+    int base = (s1 == s2) ? 13 : 91;
+    for (int r = 12; r > hi; --r) base += r;
+    return base + (hi - 1 - lo);
+}
+
+/* kernel_gen_preflop_matrix (:95-127): 3,000 LCG board samples per class pair */
+void orc_pf_allin_matrix(int hc_begin, int hc_end, float* out, int32_t* wins_out, int32_t* ties_out) {
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int hc = hc_begin; hc < hc_end; ++hc)
+        for (int vc = 0; vc < PF_CLASSES; ++vc) {
+            float* o = &out[hc * PF_CLASSES + vc];
+            if (wins_out) { wins_out[hc * PF_CLASSES + vc] = 0; ties_out[hc * PF_CLASSES + vc] = 0; }
+            if (hc == vc) { *o = 0.5f; continue; }
+            uint8_t h1, h2, v1, v2;
+            orc_pf_class_to_cards(hc, &h1, &h2);
+            orc_pf_class_to_cards(vc, &v1, &v2);
+            if (h1 == v1 || h1 == v2 || h2 == v1 || h2 == v2) {
+                if (h1 == v1 || h2 == v1) v1 = (uint8_t)((v1 / 4) * 4 + 2);
+                if (h1 == v2 || h2 == v2) v2 = (uint8_t)((v2 / 4) * 4 + 3);
+            }
+            uint64_t dead = (1ull << h1) | (1ull << h2) | (1ull << v1) | (1ull << v2);
+            uint8_t deck[52]; int dsz = 0;
+            for (int c = 0; c < 52; ++c) if (!(dead & (1ull << c))) deck[dsz++] = (uint8_t)c;
+            uint32_t rng = (uint32_t)(hc * 169 + vc) * 2654435761u + 0x9E3779B9u;
+            int wins = 0, ties = 0;
+            uint8_t a[7] = {h1, h2, 0, 0, 0, 0, 0}, b[7] = {v1, v2, 0, 0, 0, 0, 0};
+            for (int s = 0; s < 3000; ++s) {
+                uint8_t bd[5];
+                for (int k = 0; k < 5; ++k) {
+                    rng = rng * 1664525u + 1013904223u;
+                    int pick = k + (int)((rng >> 16) % (uint32_t)(dsz - k));
+                    bd[k] = deck[pick];
+                }
+                for (int k = 0; k < 5; ++k) { a[2 + k] = bd[k]; b[2 + k] = bd[k]; }
+                uint32_t sh = orc_score7(a), sv = orc_score7(b);
+                if (sh > sv) wins++; else if (sh == sv) ties++;
+            }
+            *o = ((float)wins + 0.5f * (float)ties) / 3000.0f;
+            if (wins_out) { wins_out[hc * PF_CLASSES + vc] = wins; ties_out[hc * PF_CLASSES + vc] = ties; }
+        }
+}
+
+/* The alive-combo list and per-class lists of the host set-up (:467-495):
+ * the first 1,176 combos in lexicographic order, at most 12 per class. */
+static void orc_pf_lists(uint8_t* cc /* [1176][2] */, int* cls_count /* [169] */, int* cls_idx /* [169][12] */) {
+    int n = 0;
+    for (int k = 0; k < PF_CLASSES; ++k) cls_count[k] = 0;
+    for (int c1 = 0; c1 < 52; ++c1)
+        for (int c2 = c1 + 1; c2 < 52; ++c2) {
+            if (n >= PF_ALIVE) continue;
+            int cls = orc_pf_combo_class(c1, c2);
+            cc[2 * n] = (uint8_t)c1; cc[2 * n + 1] = (uint8_t)c2;
+            if (cls_count[cls] < 12) cls_idx[cls * 12 + cls_count[cls]++] = n;
+            ++n;
+        }
+}
+
+/* kernel_gen_100_flop_matrices (:130-183) for one flop, then
+ * kernel_reduce_combo_to_class_matrices (:189-223).  Entries of hero combos
+ * that touch the flop are never written by the reference (its buffer is
+ * uninitialised); here they read as 0, which the reduction skips (eq > 0).
+ * out_class[v_cls * 169 + h_cls]. */
+void orc_pf_flop_class_matrix(const uint8_t flop[3], float* out_class, float* out_combo /* optional [1216*1216] */) {
+    uint8_t cc[2 * PF_ALIVE];
+    int cnt[PF_CLASSES], idx[PF_CLASSES * 12];
+    orc_pf_lists(cc, cnt, idx);
+    float* E = out_combo ? out_combo : (float*)malloc(sizeof(float) * PF_PADDED * PF_PADDED);
+    memset(E, 0, sizeof(float) * PF_PADDED * PF_PADDED);
+    uint64_t fm = (1ull << flop[0]) | (1ull << flop[1]) | (1ull << flop[2]);
+    #pragma omp parallel for schedule(dynamic, 8)
+    for (int h = 0; h < PF_ALIVE; ++h) {
+        uint64_t hm = (1ull << cc[2 * h]) | (1ull << cc[2 * h + 1]);
+        if (hm & fm) continue;
+        uint64_t dhf = hm | fm;
+        uint8_t deck[52]; int dsz = 0;
+        for (int c = 0; c < 52; ++c) if (!(dhf & (1ull << c))) deck[dsz++] = (uint8_t)c;
+        for (int j = 0; j < PF_ALIVE; ++j) {
+            uint64_t vm = (1ull << cc[2 * j]) | (1ull << cc[2 * j + 1]);
+            if ((hm & vm) || (vm & fm)) { E[(size_t)j * PF_PADDED + h] = 0.0f; continue; }
+            uint8_t a[7] = {flop[0], flop[1], flop[2], cc[2 * h], cc[2 * h + 1], 0, 0};
+            uint8_t b[7] = {flop[0], flop[1], flop[2], cc[2 * j], cc[2 * j + 1], 0, 0};
+            uint64_t dall = dhf | vm;
+            int wins = 0, ties = 0, total = 0;
+            for (int r1 = 0; r1 < dsz; r1 += 2) {
+                uint8_t t = deck[r1];
+                if (dall & (1ull << t)) continue;
+                a[5] = t; b[5] = t;
+                for (int r2 = r1 + 1; r2 < dsz; r2 += 3) {
+                    uint8_t r = deck[r2];
+                    if (dall & (1ull << r)) continue;
+                    a[6] = r; b[6] = r;
+                    uint32_t sh = orc_score7(a), sv = orc_score7(b);
+                    if (sh > sv) wins += 2; else if (sh == sv) ties += 1;
+                    total += 2;
+                }
+            }
+            E[(size_t)j * PF_PADDED + h] = total > 0 ? ((float)wins + 0.5f * (float)ties) / (float)total : 0.0f;
+        }
+    }
+    for (int hc = 0; hc < PF_CLASSES; ++hc)
+        for (int vc = 0; vc < PF_CLASSES; ++vc) {
+            float sum = 0.0f;
+            int valid = 0;
+            for (int i = 0; i < cnt[hc]; ++i)
+                for (int j = 0; j < cnt[vc]; ++j) {
+                    float eq = E[(size_t)idx[vc * 12 + j] * PF_PADDED + idx[hc * 12 + i]];
+                    if (eq > 0.0f) { sum += eq; valid++; }
+                }
+            out_class[vc * PF_CLASSES + hc] = valid > 0 ? sum / (float)valid : 0.5f;
+        }
+    if (!out_combo) free(E);
+}
+
+/* The closed preflop tree and DCFR loop (:224-421, :563-614): BTN root
+ * (fold / min-raise / jam), BB vs min-raise (fold / call / 3-bet jam), BTN vs
+ * 3-bet jam (fold / call), BB vs open jam (fold / call); flop play is the
+ * co-solve over the class-reduced board matrices.  class_mats: [n][v][h]. */
+
+static void orc_pf_cosolve(int nf, const float* fw, const float* rbc, const float* rbb, const float* mats,
+                           float* ev_btn, float* ev_bb, float pot_flop, float bf) {
+    for (int cls = 0; cls < PF_CLASSES; ++cls) {
+        float acc_btn = 0.0f, acc_bb = 0.0f, tw = 0.0f;
+        for (int f = 0; f < nf; ++f) {
+            float w = fw[f];
+            tw += w;
+            const float* eq = &mats[(size_t)f * PF_CLASSES * PF_CLASSES];
+            float s1 = 0.0f, e0 = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) { float r = rbb[o]; s1 += r; e0 += r * eq[o * PF_CLASSES + cls]; }
+            if (s1 > 1e-7f) e0 /= s1;
+            float s0 = 0.0f, e1 = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) { float r = rbc[o]; s0 += r; e1 += r * (1.0f - eq[cls * PF_CLASSES + o]); }
+            if (s0 > 1e-7f) e1 /= s0;
+            float sh_btn = e0 * 1.06f * pot_flop, sh_bb = e1 * 0.94f * pot_flop;
+            float nb = sh_btn >= 2.1f ? sh_btn - 2.1f : -((2.1f - sh_btn) * bf);
+            float nbb = sh_bb >= 2.1f ? sh_bb - 2.1f : -((2.1f - sh_bb) * bf);
+            acc_btn += w * nb;
+            acc_bb += w * nbb;
+        }
+        if (tw > 0.0f) { ev_btn[cls] = acc_btn / tw; ev_bb[cls] = acc_bb / tw; }
+    }
+}
+
+static void orc_pf_dcfr_step(int A, float* R, float* sig, float* S, const float* cfv, const float* reach, float wp, float ws) {
+    for (int cls = 0; cls < PF_CLASSES; ++cls) {
+        float v = 0.0f;
+        for (int a = 0; a < A; ++a) v += sig[a * PF_PAD + cls] * cfv[a * PF_PAD + cls];
+        float pos = 0.0f, nxt[3] = {0.0f, 0.0f, 0.0f};
+        for (int a = 0; a < A; ++a) {
+            int i = a * PF_PAD + cls;
+            float nr = wp * fmaxf(0.0f, R[i] + (cfv[i] - v));
+            R[i] = nr; pos += nr; nxt[a] = nr;
+            S[i] += ws * reach[cls] * sig[i];
+        }
+        for (int a = 0; a < A; ++a) sig[a * PF_PAD + cls] = pos > 1e-7f ? nxt[a] / pos : 1.0f / (float)A;
+    }
+}
+
+/* sums: 4 blocks [3|3|2|2][192] (BTN root, BB defence, BTN vs 3-bet, BB vs jam). */
+int orc_pf_dcfr(int nf, const float* flop_weights, const float* class_mats, const float* allin,
+                const orc_pf_params* p, float* sums, float* sigma) {
+    const int A[4] = {3, 3, 2, 2};
+    float *R[4], *G[4], *S[4], *C[4];
+    for (int k = 0; k < 4; ++k) {
+        R[k] = (float*)calloc((size_t)A[k] * PF_PAD, sizeof(float));
+        G[k] = (float*)calloc((size_t)A[k] * PF_PAD, sizeof(float));
+        S[k] = (float*)calloc((size_t)A[k] * PF_PAD, sizeof(float));
+        C[k] = (float*)calloc((size_t)A[k] * PF_PAD, sizeof(float));
+        for (int i = 0; i < A[k] * PF_PAD; ++i) G[k][i] = 1.0f / (float)A[k];
+    }
+    float root[PF_PAD] = {0}, rbc[PF_PAD] = {0}, rbb[PF_PAD] = {0}, evb[PF_PAD] = {0}, evbb[PF_PAD] = {0};
+    for (int c = 0; c < PF_CLASSES; ++c) root[c] = (c < 13 ? 6.0f : c < 91 ? 4.0f : 12.0f) / 1326.0f;
+    const float dead = p->dead_pot, stack = p->stack_bb, bf = p->bubble;
+    const float jam_pot = 2.0f * stack + dead;
+    for (int t = 1; t <= p->iters; ++t) {
+        float tf = (float)t;
+        float wp = powf(tf, 1.5f) / (powf(tf, 1.5f) + 1.0f), ws = tf * tf;
+        for (int c = 0; c < PF_CLASSES; ++c) {            /* kernel_update_dynamic_reaches */
+            rbc[c] = root[c] * G[0][1 * PF_PAD + c];
+            rbb[c] = root[c] * G[1][1 * PF_PAD + c];
+        }
+        orc_pf_cosolve(nf, flop_weights, rbc, rbb, class_mats, evb, evbb, dead + 3.1f, bf);
+        for (int cls = 0; cls < PF_CLASSES; ++cls) {       /* kernel_build_closed_preflop_cfvs */
+            const float *sbr = G[0], *sbd = G[1], *s3b = G[2], *sbj = G[3];
+            C[2][0 * PF_PAD + cls] = -2.1f * bf;
+            float m3 = 0.0f, eqc = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) { float r = root[o] * sbd[2 * PF_PAD + o]; m3 += r; eqc += r * allin[cls * PF_CLASSES + o]; }
+            if (m3 > 1e-7f) eqc /= m3;
+            C[2][1 * PF_PAD + cls] = eqc * (jam_pot - stack) - (1.0f - eqc) * bf * stack;
+            float v3 = s3b[0 * PF_PAD + cls] * C[2][0 * PF_PAD + cls] + s3b[1 * PF_PAD + cls] * C[2][1 * PF_PAD + cls];
+            C[1][0 * PF_PAD + cls] = -1.0f * bf;
+            C[1][1 * PF_PAD + cls] = evbb[cls];
+            float bf3 = 0.0f, bc3 = 0.0f, eqj = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) {
+                float ro = root[o] * sbr[1 * PF_PAD + o];
+                bf3 += ro * s3b[0 * PF_PAD + o];
+                bc3 += ro * s3b[1 * PF_PAD + o];
+                eqj += ro * s3b[1 * PF_PAD + o] * (1.0f - allin[o * PF_CLASSES + cls]);
+            }
+            if (bc3 > 1e-7f) eqj /= bc3;
+            float tot3 = bf3 + bc3 + 1e-9f;
+            float evsh = eqj * (jam_pot - stack) - (1.0f - eqj) * bf * stack;
+            C[1][2 * PF_PAD + cls] = (bf3 * (dead + 2.1f) + bc3 * evsh) / tot3;
+            C[3][0 * PF_PAD + cls] = -1.0f * bf;
+            float mj = 0.0f, eqo = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) { float r = root[o] * sbr[2 * PF_PAD + o]; mj += r; eqo += r * (1.0f - allin[o * PF_CLASSES + cls]); }
+            if (mj > 1e-7f) eqo /= mj;
+            C[3][1 * PF_PAD + cls] = eqo * (jam_pot - stack) - (1.0f - eqo) * bf * stack;
+            C[0][0 * PF_PAD + cls] = 0.0f;
+            float fm = 0.0f, cm = 0.0f, jm = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) {
+                float r = root[o];
+                fm += r * sbd[0 * PF_PAD + o]; cm += r * sbd[1 * PF_PAD + o]; jm += r * sbd[2 * PF_PAD + o];
+            }
+            float tb = fm + cm + jm + 1e-9f;
+            C[0][1 * PF_PAD + cls] = (fm * dead + cm * evb[cls] + jm * v3) / tb;
+            float fj = 0.0f, cj = 0.0f, eo = 0.0f;
+            for (int o = 0; o < PF_CLASSES; ++o) {
+                float r = root[o];
+                fj += r * sbj[0 * PF_PAD + o]; cj += r * sbj[1 * PF_PAD + o];
+                eo += r * sbj[1 * PF_PAD + o] * allin[cls * PF_CLASSES + o];
+            }
+            float toj = fj + cj + 1e-9f;
+            if (cj > 1e-7f) eo /= cj;
+            C[0][2 * PF_PAD + cls] = (fj * dead + cj * (eo * (jam_pot - stack) - (1.0f - eo) * bf * stack)) / toj;
+        }
+        orc_pf_dcfr_step(3, R[0], G[0], S[0], C[0], root, wp, ws);
+        orc_pf_dcfr_step(3, R[1], G[1], S[1], C[1], root, wp, ws);
+        orc_pf_dcfr_step(2, R[2], G[2], S[2], C[2], root, wp, ws);
+        orc_pf_dcfr_step(2, R[3], G[3], S[3], C[3], root, wp, ws);
+    }
+    size_t o = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (sums) memcpy(sums + o, S[k], sizeof(float) * (size_t)A[k] * PF_PAD);
+        if (sigma) memcpy(sigma + o, G[k], sizeof(float) * (size_t)A[k] * PF_PAD);
+        o += (size_t)A[k] * PF_PAD;
+        free(R[k]); free(G[k]); free(S[k]); free(C[k]);
+    }
+    return MTT_OK;
+}

@@ -117,6 +117,17 @@ int orc_mw_solve(const orc_mw_game* g, const orc_cfr_params* prm, float* R[4], f
 /* Malmuth-Harville equity by enumerating the ordered finishers of the m paid places. */
 int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, double* out);
 
+/* --- preflop anchor chain: src/preflop/preflop_grid_generator.cu ---------- */
+int  orc_pf_combo_class(int c1, int c2);
+/* 169 x 169 all-in equities out[h*169+v] (and the integer win/tie counts). */
+void orc_pf_allin_matrix(int hc_begin, int hc_end, float* out, int32_t* wins, int32_t* ties);
+/* One flop's class-reduced equity matrix out_class[v*169+h] (reference mode). */
+void orc_pf_flop_class_matrix(const uint8_t flop[3], float* out_class, float* out_combo);
+typedef struct orc_pf_params { int32_t iters; float stack_bb, bubble, dead_pot; } orc_pf_params;
+/* DCFR over the closed preflop tree; sums / sigma: [3|3|2|2][192] blocks. */
+int orc_pf_dcfr(int nf, const float* flop_weights, const float* class_mats, const float* allin,
+                const orc_pf_params* p, float* sums, float* sigma);
+
 #ifdef __cplusplus
 }
 #endif

@@ -239,3 +239,39 @@ def icm_equity(stacks, payouts):
     if L.orc_icm_equity(st.ctypes.data, len(st), pay.ctypes.data, len(pay), out.ctypes.data):
         raise RuntimeError("orc_icm_equity failed")
     return out
+
+
+class PfParams(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("stack_bb", ctypes.c_float), ("bubble", ctypes.c_float),
+                ("dead_pot", ctypes.c_float)]
+
+
+def pf_allin(hc_begin=0, hc_end=169):
+    L = lib()
+    L.orc_pf_allin_matrix.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    out = np.zeros(169 * 169, np.float32); w = np.zeros(169 * 169, np.int32); t = np.zeros(169 * 169, np.int32)
+    L.orc_pf_allin_matrix(hc_begin, hc_end, out.ctypes.data, w.ctypes.data, t.ctypes.data)
+    return out.reshape(169, 169), w.reshape(169, 169), t.reshape(169, 169)
+
+
+def pf_flop_class(flop):
+    L = lib()
+    L.orc_pf_flop_class_matrix.argtypes = [vp, vp, vp]
+    f = np.ascontiguousarray(flop, np.uint8)
+    out = np.zeros(169 * 169, np.float32)
+    L.orc_pf_flop_class_matrix(f.ctypes.data, out.ctypes.data, None)
+    return out.reshape(169, 169)
+
+
+def pf_dcfr(weights, class_mats, allin, iters=500, stack_bb=20.0, bubble=1.35, dead_pot=2.5):
+    L = lib()
+    L.orc_pf_dcfr.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp]
+    L.orc_pf_dcfr.restype = ctypes.c_int
+    w = np.ascontiguousarray(weights, np.float32)
+    m = np.ascontiguousarray(class_mats, np.float32)
+    a = np.ascontiguousarray(allin, np.float32)
+    sums = np.zeros(10 * 192, np.float32); sig = np.zeros(10 * 192, np.float32)
+    p = PfParams(int(iters), float(stack_bb), float(bubble), float(dead_pot))
+    L.orc_pf_dcfr(len(w), w.ctypes.data, m.ctypes.data, a.ctypes.data, ctypes.byref(p), sums.ctypes.data,
+                  sig.ctypes.data)
+    return sums.reshape(10, 192), sig.reshape(10, 192)

@@ -161,3 +161,27 @@ def test_continuation_matches_a_longer_solve(mtt, wl, cuda):
     for a_, r_ in zip(cont, ref):
         for k in ("R0", "R1", "S0", "S1"):
             assert np.array_equal(a_[k], r_[k]), k
+
+
+def test_config1_abstraction_small_ranges_vs_oracle(mtt, wl, orc, cuda):
+    """The turn+river tree of the DCFR workload (bets 33/75/150% + all-in,
+    2 raises on both streets, 104k nodes) with 24-combo ranges: DCFR
+    (1.5, 0, 2) against the oracle."""
+    sub = wl.turn_dcfr(seed=1, n_hands=24)
+    res, reads = _solve_gpu(mtt, [sub], iters=3, algo=1, alpha=1.5, beta=0.0, gamma=2.0, threads=256)
+    o = orc.cfr_solve(sub, 3, algo=1, alpha=1.5, beta=0.0, gamma=2.0, alternate=1)
+    _compare(sub, o, reads[0])
+
+
+def test_config1_full_solve(mtt, wl, cuda):
+    """The full turn+river DCFR workload (1,128 live combos per player):
+    exploitability falls with the iterations and ends small."""
+    sub = wl.turn_dcfr(seed=1)
+    b = mtt.RiverBatch([sub])
+    b.solve(mtt.solve_params(iters=50, algo=1, alpha=1.5, beta=0.0, gamma=2.0, threads=256), graph=True)
+    e50 = b.results()[0, 5]
+    b.solve(mtt.solve_params(iters=500, algo=1, alpha=1.5, beta=0.0, gamma=2.0, threads=256), graph=True)
+    r = b.results()[0]
+    b.close()
+    assert np.isfinite(r).all()
+    assert r[5] < e50 and r[5] < 5e-3, (e50, r[5])
