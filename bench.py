@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--target", type=float, default=1e-3, help="exploitability gate, fraction of the pot")
     ap.add_argument("--cpu-sample", type=int, default=0, help="subgames in the CPU baseline sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other", action="store_true", help="skip the other workloads' numbers")
     return ap.parse_args()
 
 
@@ -153,6 +154,113 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _event_ms(fn, stream, reps=1):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def other_configs(mtt, wl, stream):
+    """Device-timed numbers of the other workloads (one run each, after a
+    warm-up run): the single river subgame, the turn+river DCFR solve, the
+    differentiable EV over 1,024 boards, the four-player ICM river, the leaf
+    network's GEMM and training step, the preflop chain and the full flop-EV
+    dump."""
+    import torch
+    out = {}
+    # single river subgame, uniform ranges, 1,000 CFR+ iterations + FP64 exploitability
+    sub = wl.river_uniform(seed=0)
+    b = mtt.RiverBatch([sub])
+    p0 = mtt.solve_params(iters=1000, threads=256, avg_power=2.0)
+    b.solve(p0, graph=True)
+    t = _event_ms(lambda: b.solve(p0, graph=True), stream)
+    out["river_single"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
+                           "workload": "river, uniform 1,081-combo ranges, pot 100, stack 200, bets 50/100% + all-in, "
+                                       "1 raise, 1,000 alternating CFR+ iterations + FP64 best response"}
+    b.close()
+    # turn + river DCFR
+    sub = wl.turn_dcfr(seed=1)
+    b = mtt.RiverBatch([sub])
+    p1 = mtt.solve_params(iters=500, algo=mtt.ALGO_DCFR, alpha=1.5, beta=0.0, gamma=2.0, threads=256)
+    b.solve(mtt.solve_params(iters=5, algo=mtt.ALGO_DCFR, threads=256), graph=True)
+    t = _event_ms(lambda: b.solve(p1, graph=True), stream)
+    out["turn_river_dcfr"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
+                              "nodes": int(len(sub["nodes"])), "iter_bytes": b.info()["iter_bytes"],
+                              "workload": "turn board, 48 rivers, Dirichlet(0.3) ranges (1,128 live combos), pot 60, "
+                                          "stack 470, bets 33/75/150% + all-in, 2 raises, DCFR(1.5, 0, 2) x 500"}
+    b.close()
+    # differentiable EV of softmax strategies
+    dv = importlib.import_module("mtt-gpu-solver_b200.diffev")
+    subs, logits = wl.diff_boards(n=1024, seed=3)
+    sev = dv.StrategyEV(subs)
+    L = torch.randn(sev.total_rows, device="cuda")
+    R = torch.zeros(sev.total_range, device="cuda")
+    for s_, g in enumerate(subs):
+        o = int(sev.range_off[s_]); H = len(g["combos0"]); Hp = (H + 3) // 4 * 4
+        R[o:o + H] = torch.from_numpy(g["range0"]).to("cuda")
+        R[o + Hp:o + Hp + H] = torch.from_numpy(g["range1"]).to("cuda")
+    sev.batch.ev_grad(L, R)
+    t = _event_ms(lambda: sev.batch.ev_grad(L, R), stream)
+    out["diff_ev"] = {"ms": t, "boards_per_s": 1024 / (t * 1e-3),
+                      "workload": "1,024 river boards, config-0 trees, N(0,1) logits: root EV + adjoint (range and "
+                                  "logit gradients)"}
+    sev.close()
+    # four-player ICM river
+    mw = importlib.import_module("mtt-gpu-solver_b200.multiway")
+    sub = wl.multiway_icm(seed=4)
+    mb = mw.MultiwayBatch([sub])
+    p4 = mtt.solve_params(iters=200)
+    mb.solve(p4, graph=True)
+    t = _event_ms(lambda: mb.solve(p4, graph=True), stream)
+    out["multiway_icm"] = {"ms": t, "nodes": int(len(sub["nodes"])), "values": mb.values()[0].tolist(),
+                           "workload": "4 players, 1,081 combos, Dirichlet(0.3) ranges, Malmuth-Harville bubble "
+                                       "factors (50/30/20 over 8 seats), 200 CFR+ iterations"}
+    mb.close()
+    # leaf network: one GEMM of the first layer and one training step of 4,096 samples
+    ln = importlib.import_module("mtt-gpu-solver_b200.leafnet")
+    A = torch.randn(4096, 2752, device="cuda").to(torch.bfloat16)
+    B = torch.randn(1024, 2752, device="cuda").to(torch.bfloat16)
+    C = torch.empty(4096, 1024, device="cuda")
+    mtt.gemm_bf16(A, B, out=C)
+    t = _event_ms(lambda: mtt.gemm_bf16(A, B, out=C), stream, reps=20)
+    flops = 2.0 * 4096 * 1024 * 2752
+    out["leaf_gemm"] = {"ms": t, "tflops": flops / (t * 1e-3) / 1e12, "shape": [4096, 1024, 2752]}
+    net = ln.LeafNet(batch_cap=4096, seed=0)
+    X = torch.randn(4096, 2706, device="cuda") * 0.5
+    T = torch.randn(4096, 2652, device="cuda") * 0.3
+    net.train_step(X, T, lr=1e-4, want_loss=False)
+    t = _event_ms(lambda: net.train_step(X, T, lr=1e-4, want_loss=False), stream, reps=5)
+    out["leaf_train_step"] = {"ms": t, "samples_per_s": 4096 / (t * 1e-3),
+                              "tflops": 3 * 15.17e6 * 4096 / (t * 1e-3) / 1e12,
+                              "workload": "4,096 samples, 2,706 -> 3 x 1,024 -> 2,652, BF16 tcgen05 GEMMs + Adam"}
+    net.close()
+    # preflop chain
+    pf = importlib.import_module("mtt-gpu-solver_b200.preflop")
+    flops, w = pf.read_subset(os.path.join(ROOT, "tests", "golden", "mtt_subset.bin"))
+
+    def chain():
+        allin = pf.allin_matrix(pf.REFERENCE)
+        mats = pf.flop_class_matrices(flops, pf.REFERENCE)
+        pf.dcfr(w, mats, allin, iters=500)
+    chain()
+    out["preflop_chain"] = {"ms": _event_ms(chain, stream),
+                            "workload": "169x169 all-in matrix (3,000 samples/pair) + 100 class-reduced flop matrices "
+                                        "+ 500 DCFR iterations (reference mode)"}
+    # full flop-EV dump
+    f4 = torch.from_numpy(np.ascontiguousarray(mtt.canonical_flops()[:, :3])).to("cuda")
+    mtt.ev_dump(f4[:8])
+    out["ev_dump_1755"] = {"ms": _event_ms(lambda: mtt.ev_dump(f4), stream),
+                           "workload": "all 1,755 canonical flops, reference runout subsample (bit-exact dump)"}
+    return out
 
 
 def run_b200(args, rank, world, local):
@@ -276,6 +384,8 @@ def run_b200(args, rank, world, local):
     torch.cuda.synchronize()
     evals_per_s = 5 * 133784560 / (v0.elapsed_time(v1) * 1e-3)
 
+    other = {} if args.no_other else other_configs(mtt, wl, stream)
+
     value = args.subgames * world / (ms * 1e-3)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -305,7 +415,8 @@ def run_b200(args, rank, world, local):
             "clocks": clocks,
             "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(args.subgames * 6 * 8)},
-            "gpu_launches": int(gpu_launches)}
+            "gpu_launches": int(gpu_launches),
+            "other_configs": other}
     if rank == 0 and not args.no_cpu_baseline:
         v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, args.cpu_sample or max(os.cpu_count() or 1, 8))
         line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}

@@ -37,11 +37,15 @@ constexpr int NC = 169, PAD = 192, ALIVE = 1176, NPAIR = 1176;   // NPAIR = C(49
 constexpr int LD_REF = 1216, LD_OK = 1344;   // row length of the combo matrices (reference: 1,216)
 constexpr int SAMPLES = 3000;
 
-// class_to_cards of the reference (:79-92), boundary behaviour included.
+// class_to_cards of the reference (:79-92), boundary behaviour included: the
+// last class of each rank group maps into the next group (A2s becomes two
+// copies of the king of clubs).  For classes 90 and 168 the reference's loop
+// only ends in signed overflow (undefined); those take their own cards.
 __host__ __device__ inline void class_cards_ref(int cls, int& h1, int& h2) {
     if (cls < 13) { const int r = 12 - cls; h1 = r * 4; h2 = r * 4 + 1; return; }
     int base = cls < 91 ? 13 : 91, r1 = 12;
-    while (base + (r1 - 1) <= cls) base += r1--;
+    while (r1 > 0 && base + (r1 - 1) <= cls) base += r1--;
+    if (r1 == 0) { h1 = 4; h2 = cls < 91 ? 0 : 1; return; }
     const int r2 = r1 - 1 - (cls - base);
     h1 = r1 * 4;
     h2 = r2 * 4 + (cls < 91 ? 0 : 1);

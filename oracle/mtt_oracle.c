@@ -976,12 +976,18 @@ int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, do
 #define PF_ALIVE 1176
 #define PF_PADDED 1216
 
-/* class_to_cards (:79-92), including its boundary behaviour */
+/* class_to_cards (:79-92), including its boundary behaviour: the last class
+ * of each rank group maps to the next group (e.g. A2s to two copies of the
+ * king of clubs).  For the last suited and the last offsuit class (90, 168)
+ * the reference's loop never leaves through its condition (it runs into
+ * signed overflow, undefined behaviour); there the class's own cards
+ * (3c2c, 3c2d) are used. */
 static void orc_pf_class_to_cards(int cls, uint8_t* h1, uint8_t* h2) {
     if (cls < 13) { int r = 12 - cls; *h1 = (uint8_t)(r * 4 + 0); *h2 = (uint8_t)(r * 4 + 1); }
     else {
         int base = cls < 91 ? 13 : 91, r1 = 12, r2;
-        while (base + (r1 - 1) <= cls) base += r1--;
+        while (r1 > 0 && base + (r1 - 1) <= cls) base += r1--;
+        if (r1 == 0) { *h1 = 4; *h2 = (uint8_t)(cls < 91 ? 0 : 1); return; }
         r2 = r1 - 1 - (cls - base);
         *h1 = (uint8_t)(r1 * 4 + 0);
         *h2 = (uint8_t)(r2 * 4 + (cls < 91 ? 0 : 1));
