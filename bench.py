@@ -46,6 +46,22 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, pg, device):
+    """The largest of the ranks' values of x (the job's time is its slowest
+    replica's); x itself without a process group."""
+    if pg is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(seed, rank):
+    """Seed of a rank's own batch: replicas solve different subgames."""
+    return seed + 1000 * rank
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -274,7 +290,7 @@ def run_b200(args, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    subs = wl.river_batch(n=args.subgames, seed=args.seed + 1000 * rank)
+    subs = wl.river_batch(n=args.subgames, seed=replica_seed(args.seed, rank))
     # 1,000 alternating CFR+ iterations per subgame, then the FP64 best
     # response; subgames still above 0.1% of the pot continue in chunks of 500
     # iterations (compacted work lists) until they pass, up to 4x the budget
@@ -308,10 +324,7 @@ def run_b200(args, rank, world, local):
     gpu_launches = batch.launch_count() - launches0
     clocks = clk.stop()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, pg, "cuda")
     res = batch.results()
     expl = res[:, 5]
     its = batch.iterations()
@@ -353,10 +366,7 @@ def run_b200(args, rank, world, local):
     for _ in range(max(1, min(args.steps, 2))):
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
-    if pg:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, pg, "cuda")
     h2d = sum(g["nodes"].nbytes + g["combos0"].nbytes + g["combos1"].nbytes + g["range0"].nbytes +
               g["range1"].nbytes for g in subs)
 

@@ -316,8 +316,9 @@ int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, vo
 #define MTT_LEAF_HIDDEN 1024
 #define MTT_LEAF_OUT    2652
 typedef struct mtt_leafnet mtt_leafnet;
+#define MTT_LEAF_ZERO_OUTPUT 1   /* flags: start the output layer at zero (a residual on a base estimate) */
 /* batch_cap: largest batch (multiple of 8).  He-initialised from seed. */
-int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, mtt_leafnet** out);
+int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, int32_t flags, mtt_leafnet** out);
 /* d_x [M][2706] float features -> d_y [M][2652] float predictions. */
 int mtt_leafnet_forward(mtt_leafnet* n, const float* d_x, int32_t M, float* d_y, void* stream);
 /* Gradients of the masked mean squared error sum(w (y - t)^2) / (M * 2652)

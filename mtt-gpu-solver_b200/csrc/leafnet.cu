@@ -245,7 +245,7 @@ int backward(mtt_leafnet* n, const float* d_y, const float* d_w, int M, double n
 }
 }  // namespace
 
-extern "C" int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, mtt_leafnet** out) {
+extern "C" int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, int32_t flags, mtt_leafnet** out) {
     if (!out || batch_cap < 1 || batch_cap > (1 << 20) || (batch_cap % 8)) return MTT_ERR_INVALID;
     *out = nullptr;
     mtt_leafnet* n = new mtt_leafnet();
@@ -267,7 +267,8 @@ extern "C" int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, mtt_leafnet*
         const size_t cnt = (size_t)L.in * L.out;
         std::vector<float> w(cnt, 0.0f);
         std::vector<unsigned char> live(cnt, 0);
-        const double sd = std::sqrt(2.0 / (double)L.in_live);   // He initialisation
+        // He initialisation; the output layer starts at zero when asked
+        const double sd = (l == NL - 1 && (flags & MTT_LEAF_ZERO_OUTPUT)) ? 0.0 : std::sqrt(2.0 / (double)L.in_live);
         for (int o = 0; o < L.out_live; ++o)
             for (int i = 0; i < L.in_live; ++i) {
                 const double u1 = urand(), u2 = urand();

@@ -136,8 +136,8 @@ __device__ __forceinline__ TermInfo term_info(const SubDesc& sd, const DNode& nd
 }
 
 // Shared scratch of one terminal CTA, in elements of the arithmetic type.
-// Ho + 8 staged reach, then 3 Ho + 1 prefix values and 2 x 52 per-card values.
-__host__ __device__ constexpr int term_scratch(int max_h) { return 4 * max_h + 128; }
+// Ho + 8 staged reach, then 3 Ho + 1 prefix values.
+__host__ __device__ constexpr int term_scratch(int max_h) { return 4 * max_h + 96; }
 constexpr int TT = 128;   // threads per terminal CTA (fixed: results never depend on it changing)
 
 template <typename TA, int NT = TT>
@@ -176,7 +176,9 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     const int lane = tid & 31, wid = tid >> 5;
     // opponent reach: already in shared memory (STAGED), else staged here with coalesced loads
     TA* Rd = X;
-    TA* Xs = STAGED ? X : X + Ho + 8;   // scan region: 3*Ho + 1 prefix values, then 2 x 52 per-card values
+    TA* Xs = STAGED ? X : X + Ho + 8;   // scan region: 3*Ho + 1 prefix values
+    __shared__ TA cB[52], cE[52];       // per card: prefix at the start / end of its list (folds: cB = card sums)
+    __shared__ int cS[52];              // per card: scan index of its list's start
     if (!STAGED) {
 #pragma unroll 4
         for (int j = tid; j < Ho; j += NT) Rd[j] = (TA)ro[j];
@@ -190,7 +192,7 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         for (int j = tid; j < Ho; j += NT) part += Rs(j);
         const TA tot = cta_sum<TA, NT>(part, wb, tid);
         // opponent reach holding each card: one warp per card, lane-strided
-        TA* Cs = Xs;
+        TA* Cs = cB;
         for (int c = wid; c < 52; c += NT / 32) {
             TA sm = TA(0);
             for (int e = seg[c] + lane; e < seg[c + 1]; e += 32) sm += Rs(co[e]);
@@ -247,12 +249,12 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     }
     if (tid == 0) Xs[N] = total;
     __syncthreads();
-    // per card: the prefix at the start and at the end of its list
-    TA* Bc = Xs + N + 1;
-    TA* Ec = Bc + 52;
+    // per card: the scan index of its list and the prefix at its start and end
     for (int c = tid; c < 52; c += NT) {
-        Bc[c] = Xs[Ho + seg[c]];
-        Ec[c] = Xs[Ho + seg[c + 1]];
+        const int a = Ho + seg[c];
+        cS[c] = a;
+        cB[c] = Xs[a];
+        cE[c] = Xs[Ho + seg[c + 1]];
     }
     __syncthreads();
     const TA Tt = Xs[Ho];
@@ -261,11 +263,12 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         if (h < Hq) {
             const Entry et = ent[h];
             if (et.lt != 0xFFFFu) {
-                const TA b1 = Bc[et.c1], b2 = Bc[et.c2];
-                const TA C1 = Ec[et.c1] - b1, C2 = Ec[et.c2] - b2;
+                const int s1c = cS[et.c1], s2c = cS[et.c2];
+                const TA b1 = cB[et.c1], b2 = cB[et.c2];
+                const TA C1 = cE[et.c1] - b1, C2 = cE[et.c2] - b2;
                 const TA ps = et.same >= 0 ? Rs(et.same) : TA(0);
-                const TA W = Xs[et.lt] - (Xs[et.i1lt] - b1) - (Xs[et.i2lt] - b2);
-                const TA LE = Xs[et.le] - (Xs[et.i1le] - b1) - (Xs[et.i2le] - b2);
+                const TA W = Xs[et.lt] - (Xs[s1c + et.ltc1] - b1) - (Xs[s2c + et.ltc2] - b2);
+                const TA LE = Xs[et.le] - (Xs[s1c + et.lec1] - b1) - (Xs[s2c + et.lec2] - b2);
                 const TA Ti = LE - W + ps;
                 if (!semantics) {
                     const TA L = Tt - C1 - C2 - LE;
@@ -487,7 +490,7 @@ __host__ __device__ inline int tg_scan_doubles(int H0, int H1, int upd) {
     for (int q = 0; q < 2; ++q) {
         if (!((upd >> q) & 1)) continue;
         const int Ho = q ? H0 : H1;
-        const int need = 3 * Ho + 112;   // prefix values (3 Ho + 1) and the per-card tables (2 x 52)
+        const int need = 3 * Ho + 8;     // prefix values (3 Ho + 1)
         m = need > m ? need : m;
     }
     return m;

@@ -45,9 +45,10 @@ _CARDS = np.array([(a, b) for a in range(52) for b in range(a + 1, 52)], np.int6
 
 
 class LeafNet:
-    def __init__(self, batch_cap=4096, seed=0):
+    def __init__(self, batch_cap=4096, seed=0, zero_output=False):
         h = ctypes.c_void_p()
-        check("mtt_leafnet_create", lib().mtt_leafnet_create(int(batch_cap), int(seed), ctypes.byref(h)))
+        check("mtt_leafnet_create", lib().mtt_leafnet_create(int(batch_cap), int(seed), 1 if zero_output else 0,
+                                                             ctypes.byref(h)))
         self._h = h
         self.cap = batch_cap
 
@@ -158,19 +159,35 @@ def river_training_set(n, seed=0, iters=300, batch=2048, spr=(0.5, 1.0, 2.0, 3.0
     return X, T, W, meta
 
 
-def checkdown_values(meta, device="cuda"):
+def checkdown_values(meta, batch=4096):
     """The leaf estimate without a network: both players check the river
-    down; per combo 0.5 * sum_j r_opp(j) (win - loss) in units of the pot,
-    from the GPU showdown counts.  Returns [n, 2652] like the targets."""
-    import torch
-    from . import board_showdown_counts
-    hands = torch.from_numpy(_CARDS.astype(np.uint8)).to(device)
+    down.  Per combo, the showdown value against the opponent's range with
+    card removal and split ties, in units of the pot (ranges summing to 1),
+    from the solver's own FP64 terminal pass on a one-node showdown tree.
+    Returns [n, 2652] like the targets (0 for combos touching the board)."""
+    from . import NODE_DTYPE, NODE_SHOWDOWN, RiverBatch, solve_params
+    node = np.zeros(1, dtype=NODE_DTYPE)
+    node[0]["type"] = NODE_SHOWDOWN
+    node[0]["pot_size"] = 100.0
+    node[0]["committed"] = [50.0, 50.0]
+    node[0]["turn_idx"] = -1
     out = np.zeros((len(meta), OUT), np.float32)
-    for i, m in enumerate(meta):
-        Wc, Tc, Lc = board_showdown_counts(torch.tensor(m["board"], dtype=torch.uint8, device=device), hands)
-        D = (Wc - Lc).double()
-        r0 = torch.from_numpy(m["range0"]).to(device)
-        r1 = torch.from_numpy(m["range1"]).to(device)
-        out[i, :1326] = (0.5 * (D @ r1)).cpu().numpy()
-        out[i, 1326:] = (0.5 * (D @ r0)).cpu().numpy()
+    for b0 in range(0, len(meta), batch):
+        subs = []
+        for m in meta[b0:b0 + batch]:
+            live = np.nonzero(_live_mask(m["board"]))[0]
+            g = {"nodes": node, "rows": (0, 0), "board": m["board"], "pot": 100.0}
+            for p in range(2):
+                r = np.asarray(m[f"range{p}"], np.float64)[live]
+                g[f"combos{p}"] = live.astype(np.uint16)
+                g[f"range{p}"] = (r / r.sum()).astype(np.float32) if r.sum() > 0 else r.astype(np.float32)
+            subs.append(g)
+        rb = RiverBatch(subs)
+        rb.solve(solve_params(iters=0, exploitability=True))
+        for k, g in enumerate(subs):
+            ev0, ev1, _, _ = rb.root_values(k)
+            c = g["combos0"].astype(np.int64)
+            out[b0 + k, c] = (ev0 / 100.0).astype(np.float32)
+            out[b0 + k, 1326 + c] = (ev1 / 100.0).astype(np.float32)
+        rb.close()
     return out
