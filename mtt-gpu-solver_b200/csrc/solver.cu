@@ -136,7 +136,6 @@ __device__ __forceinline__ TermInfo term_info(const SubDesc& sd, const DNode& nd
 }
 
 // Shared scratch of one terminal CTA, in elements of the arithmetic type.
-// Ho + 8 staged reach, then 3 Ho + 1 prefix values.
 __host__ __device__ constexpr int term_scratch(int max_h) { return 4 * max_h + 96; }
 constexpr int TT = 128;   // threads per terminal CTA (fixed: results never depend on it changing)
 
@@ -173,12 +172,9 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     const TA cq = (TA)ti.c[q];
     const TA pot = (TA)ti.pot;
     const TA gain = pot - cq, loss = -cq, tie = TA(0.5) * pot - cq;
-    const int lane = tid & 31, wid = tid >> 5;
     // opponent reach: already in shared memory (STAGED), else staged here with coalesced loads
     TA* Rd = X;
-    TA* Xs = STAGED ? X : X + Ho + 8;   // scan region: 3*Ho + 1 prefix values
-    __shared__ TA cB[52], cE[52];       // per card: prefix at the start / end of its list (folds: cB = card sums)
-    __shared__ int cS[52];              // per card: scan index of its list's start
+    TA* Xs = STAGED ? X : X + Ho + 8;   // scan region (3*Ho + 1) / fold: per-card order + card sums
     if (!STAGED) {
 #pragma unroll 4
         for (int j = tid; j < Ho; j += NT) Rd[j] = (TA)ro[j];
@@ -191,13 +187,14 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         TA part = TA(0);
         for (int j = tid; j < Ho; j += NT) part += Rs(j);
         const TA tot = cta_sum<TA, NT>(part, wb, tid);
-        // opponent reach holding each card: one warp per card, lane-strided
-        TA* Cs = cB;
-        for (int c = wid; c < 52; c += NT / 32) {
+        TA* Cs = Xs + 2 * Ho + 8;
+#pragma unroll 4
+        for (int e = tid; e < 2 * Ho; e += NT) Xs[e] = Rs(co[e]);
+        __syncthreads();
+        for (int c = tid; c < 52; c += NT) {
             TA sm = TA(0);
-            for (int e = seg[c] + lane; e < seg[c + 1]; e += 32) sm += Rs(co[e]);
-            sm = warp_sum(sm);
-            if (lane == 0) Cs[c] = sm;
+            for (int e = seg[c]; e < seg[c + 1]; ++e) sm += Xs[e];
+            Cs[c] = sm;
         }
         __syncthreads();
         for (int h = tid; h < Hpq; h += NT) {
@@ -216,15 +213,17 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         __syncthreads();
         return;
     }
-    // showdown: exclusive scan of the opponent reach in [rank order | per-card
-    // rank orders]; each thread gathers its own chunk twice (sum, then prefix)
+    // showdown: Xs = [reach in rank order | reach in per-card rank order], exclusive scan
     const uint16_t* so = tv.sorted[o];
     const int N = 3 * Ho;
-    auto src = [&](int k) -> TA { return Rs(k < Ho ? so[k] : co[k - Ho]); };
+#pragma unroll 4
+    for (int k = tid; k < N; k += NT) Xs[k] = Rs(k < Ho ? so[k] : co[k - Ho]);
+    __syncthreads();
     const int C = ((N + NT - 1) / NT) | 1;   // odd chunk: conflict-free strides
     const int s0 = min(tid * C, N), s1 = min(s0 + C, N);
     TA loc = TA(0);
-    for (int k = s0; k < s1; ++k) loc += src(k);
+    for (int k = s0; k < s1; ++k) loc += Xs[k];
+    const int lane = tid & 31, wid = tid >> 5;
     TA inc = loc;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -243,19 +242,11 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
     }
     run += base;
     for (int k = s0; k < s1; ++k) {
-        const TA v = src(k);
+        const TA v = Xs[k];
         Xs[k] = run;
         run += v;
     }
     if (tid == 0) Xs[N] = total;
-    __syncthreads();
-    // per card: the scan index of its list and the prefix at its start and end
-    for (int c = tid; c < 52; c += NT) {
-        const int a = Ho + seg[c];
-        cS[c] = a;
-        cB[c] = Xs[a];
-        cE[c] = Xs[Ho + seg[c + 1]];
-    }
     __syncthreads();
     const TA Tt = Xs[Ho];
     for (int h = tid; h < Hpq; h += NT) {
@@ -263,9 +254,10 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         if (h < Hq) {
             const Entry et = ent[h];
             if (et.lt != 0xFFFFu) {
-                const int s1c = cS[et.c1], s2c = cS[et.c2];
-                const TA b1 = cB[et.c1], b2 = cB[et.c2];
-                const TA C1 = cE[et.c1] - b1, C2 = cE[et.c2] - b2;
+                const int s1c = Ho + seg[et.c1], s2c = Ho + seg[et.c2];
+                const TA b1 = Xs[s1c], b2 = Xs[s2c];
+                const TA C1 = Xs[Ho + seg[et.c1 + 1]] - b1, C2 = Xs[Ho + seg[et.c2 + 1]] - b2;
+ 
                 const TA ps = et.same >= 0 ? Rs(et.same) : TA(0);
                 const TA W = Xs[et.lt] - (Xs[s1c + et.ltc1] - b1) - (Xs[s2c + et.ltc2] - b2);
                 const TA LE = Xs[et.le] - (Xs[s1c + et.lec1] - b1) - (Xs[s2c + et.lec2] - b2);
@@ -490,7 +482,7 @@ __host__ __device__ inline int tg_scan_doubles(int H0, int H1, int upd) {
     for (int q = 0; q < 2; ++q) {
         if (!((upd >> q) & 1)) continue;
         const int Ho = q ? H0 : H1;
-        const int need = 3 * Ho + 8;     // prefix values (3 Ho + 1)
+        const int need = (3 * Ho + 8) > (2 * Ho + 64) ? (3 * Ho + 8) : (2 * Ho + 64);
         m = need > m ? need : m;
     }
     return m;
@@ -501,7 +493,7 @@ __host__ __device__ inline int tg_smem_bytes(int H0, int H1, int Hp0, int Hp1, i
 
 // Terminal values of the updated players (kernel_evaluate_terminals,
 // honest_multistreet_solver.cu:128-196), one terminal group per CTA.
-__global__ void __launch_bounds__(TG, 4) k_term(SolveDev a, const TermGroup* __restrict__ groups,
+__global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __restrict__ groups,
                                              const TermItem* __restrict__ items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s

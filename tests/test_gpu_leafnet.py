@@ -85,9 +85,9 @@ def test_trained_net_improves_on_check_down_leaves_and_beats_solving_time(ln, mt
     estimate must come far faster than solving the subgames it replaces."""
     import time
     import torch
-    n_train, n_val = 2560, 512
+    n_train, n_val = 16384, 2048
     t0 = time.perf_counter()
-    X, T, W, meta = ln.river_training_set(n_train + n_val, seed=5, iters=150, batch=1536)
+    X, T, W, meta = ln.river_training_set(n_train + n_val, seed=5, iters=150, batch=4096)
     solve_s = (time.perf_counter() - t0) / (n_train + n_val)
     t1 = time.perf_counter()
     CD = ln.checkdown_values(meta)
@@ -98,10 +98,10 @@ def test_trained_net_improves_on_check_down_leaves_and_beats_solving_time(ln, mt
     net = ln.LeafNet(batch_cap=n_val, seed=1, zero_output=True)
     rng = np.random.default_rng(0)
     first = last = None
-    for epoch in range(12):
+    for epoch in range(3):
         perm = torch.from_numpy(rng.permutation(n_train)).to(cuda)
-        for k in range(0, n_train, 256):
-            idx = perm[k:k + 256]
+        for k in range(0, n_train, 512):
+            idx = perm[k:k + 512]
             loss = net.train_step(Xt[idx].contiguous(), Rt[idx].contiguous(), Wt[idx].contiguous(), lr=1e-4)
             first = loss if first is None else first
             last = loss
