@@ -337,6 +337,15 @@ int mtt_leafnet_params(mtt_leafnet* n, int32_t layer, float* h_w, float* h_b, fl
 /* MTT_ERR_TIMEOUT if a bounded wait in the network's GEMMs gave up. */
 int mtt_leafnet_check(mtt_leafnet* n);
 int mtt_leafnet_destroy(mtt_leafnet* n);
+/* Check-down leaf values, the estimate the leaf network corrects: for n river
+ * boards (d_boards [n][5]) and both players' ranges over the 1,326 combos
+ * (d_range0, d_range1 [n][1326], each summing to 1 over the combos that avoid
+ * the board), d_out[b][p][h] = the value of player p's combo h in units of
+ * the pot when both check the river down: half of the opponent's compatible
+ * mass below it minus half of the mass above it (card removal, split ties).
+ * Combos touching the board get 0.  No reference counterpart. */
+int mtt_checkdown_values(const uint8_t* d_boards, const float* d_range0, const float* d_range1, int32_t n,
+                         float* d_out, void* stream);
 
 /* ------------------------------------------------- preflop anchor chain */
 #define MTT_PF_REFERENCE 0   /* the reference's arithmetic, quirks included (see preflop.cu) */

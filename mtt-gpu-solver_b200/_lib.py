@@ -124,6 +124,7 @@ def lib():
         "mtt_leafnet_params": ([vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_leafnet_check": ([vp], ctypes.c_int),
         "mtt_leafnet_destroy": ([vp], ctypes.c_int),
+        "mtt_checkdown_values": ([vp, vp, vp, i32, vp, vp], ctypes.c_int),
         "mtt_pf_allin_matrix": ([i32, vp, vp, vp, vp], ctypes.c_int),
         "mtt_pf_flop_class_matrices": ([i32, vp, i32, vp, vp], ctypes.c_int),
         "mtt_pf_dcfr": ([vp, vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),

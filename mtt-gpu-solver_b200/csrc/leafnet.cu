@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "mtt_common.h"
+#include "mtt_device.cuh"
 
 namespace mtt {
 int gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
@@ -380,5 +381,75 @@ extern "C" int mtt_leafnet_destroy(mtt_leafnet* n) {
     if (!n) return MTT_ERR_INVALID;
     cudaDeviceSynchronize();
     free_net(n);
+    return MTT_OK;
+}
+
+// ------------------------------------------------------------ check-down leaves
+// The leaf estimate without a network: both players check the river down.
+// Value of combo h of player p in units of the pot, with both players having
+// put in half of it: 0.5 * sum over the opponent's combos j that share no
+// card with h or the board of r_opp(j) * sign(score(h) - score(j)).  One CTA
+// per subgame; every opponent combo is read by all lanes at once (broadcast
+// from shared memory), and each hand sums its opponents in the same order, so
+// the result is deterministic.
+namespace mtt {
+namespace leaf {
+constexpr int NCOMBO = 1326;
+
+__global__ void __launch_bounds__(256) k_checkdown(const uint8_t* __restrict__ boards, const float* __restrict__ r0,
+                                                   const float* __restrict__ r1, int n, float* __restrict__ out) {
+    __shared__ uint16_t key[NCOMBO];
+    __shared__ unsigned long long msk[NCOMBO];
+    __shared__ float ro[NCOMBO];
+    const int b = blockIdx.x;
+    if (b >= n) return;
+    const uint8_t* bd = boards + 5 * (size_t)b;
+    uint64_t bm = 0;
+    for (int k = 0; k < 5; ++k) bm |= 1ull << bd[k];
+    for (int h = threadIdx.x; h < NCOMBO; h += blockDim.x) {
+        int c1 = 0, r = h, row = 51;
+        while (r >= row) { r -= row; ++c1; --row; }
+        const int c2 = c1 + 1 + r;
+        const uint64_t m = (1ull << c1) | (1ull << c2);
+        msk[h] = m;
+        uint16_t k = 0xFFFFu;                     // combos touching the board take no part
+        if (!(m & bm)) {
+            Planes p; planes_clear(p);
+            for (int i = 0; i < 5; ++i) planes_add(p, bd[i]);
+            planes_add(p, c1); planes_add(p, c2);
+            k = (uint16_t)key_planes(p);
+        }
+        key[h] = k;
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+        __syncthreads();
+        const float* rg = (dir == 0 ? r1 : r0) + (size_t)b * NCOMBO;   // the opponent's range
+        for (int j = threadIdx.x; j < NCOMBO; j += blockDim.x) ro[j] = key[j] == 0xFFFFu ? 0.0f : rg[j];
+        __syncthreads();
+        float* o = out + ((size_t)b * 2 + dir) * NCOMBO;
+        for (int h = threadIdx.x; h < NCOMBO; h += blockDim.x) {
+            const uint16_t kh = key[h];
+            float acc = 0.0f;
+            if (kh != 0xFFFFu) {
+                const uint64_t mh = msk[h];
+                for (int j = 0; j < NCOMBO; ++j) {
+                    const uint16_t kj = key[j];
+                    const float w = (msk[j] & mh) ? 0.0f : ro[j];
+                    acc += kh > kj ? w : (kh < kj ? -w : 0.0f);
+                }
+            }
+            o[h] = 0.5f * acc;
+        }
+    }
+}
+}  // namespace leaf
+}  // namespace mtt
+
+extern "C" int mtt_checkdown_values(const uint8_t* d_boards, const float* d_range0, const float* d_range1, int32_t n,
+                                    float* d_out, void* stream) {
+    if (n < 0 || (n > 0 && (!d_boards || !d_range0 || !d_range1 || !d_out))) return MTT_ERR_INVALID;
+    if (n == 0) return MTT_OK;
+    mtt::leaf::k_checkdown<<<n, 256, 0, as_stream(stream)>>>(d_boards, d_range0, d_range1, n, d_out);
+    MTT_CHECK_LAUNCH();
     return MTT_OK;
 }

@@ -159,12 +159,33 @@ def river_training_set(n, seed=0, iters=300, batch=2048, spr=(0.5, 1.0, 2.0, 3.0
     return X, T, W, meta
 
 
-def checkdown_values(meta, batch=4096):
+def checkdown_values(meta, device="cuda", stream=None):
     """The leaf estimate without a network: both players check the river
     down.  Per combo, the showdown value against the opponent's range with
     card removal and split ties, in units of the pot (ranges summing to 1),
-    from the solver's own FP64 terminal pass on a one-node showdown tree.
-    Returns [n, 2652] like the targets (0 for combos touching the board)."""
+    from the batched GPU kernel (mtt_checkdown_values).  Returns [n, 2652]
+    like the targets (0 for combos touching the board)."""
+    import torch
+    n = len(meta)
+    boards = np.asarray([m["board"] for m in meta], np.uint8).reshape(n, 5)
+    r = [np.zeros((n, 1326), np.float32), np.zeros((n, 1326), np.float32)]
+    for i, m in enumerate(meta):
+        live = _live_mask(m["board"])
+        for p in range(2):
+            v = np.asarray(m[f"range{p}"], np.float64) * live
+            r[p][i] = v / v.sum() if v.sum() > 0 else v
+    db = torch.from_numpy(boards).to(device)
+    d0, d1 = torch.from_numpy(r[0]).to(device), torch.from_numpy(r[1]).to(device)
+    out = torch.empty((n, OUT), dtype=torch.float32, device=device)
+    check("mtt_checkdown_values", lib().mtt_checkdown_values(
+        ctypes.c_void_p(db.data_ptr()), ctypes.c_void_p(d0.data_ptr()), ctypes.c_void_p(d1.data_ptr()), n,
+        ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+    return out.cpu().numpy()
+
+
+def checkdown_values_fp64(meta, batch=4096):
+    """The same check-down values from the solver's FP64 terminal pass on a
+    one-node showdown tree (slower: every board is packed on the host)."""
     from . import NODE_DTYPE, NODE_SHOWDOWN, RiverBatch, solve_params
     node = np.zeros(1, dtype=NODE_DTYPE)
     node[0]["type"] = NODE_SHOWDOWN

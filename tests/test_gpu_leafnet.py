@@ -121,3 +121,21 @@ def test_trained_net_improves_on_check_down_leaves_and_beats_solving_time(ln, mt
     assert mae_net < mae_cd < mae_zero
     assert (infer_s + cd_s) * 5 < solve_s
     net.close()
+
+
+def test_checkdown_kernel_matches_the_solver_terminal_pass(ln, mtt, cuda):
+    """The batched check-down kernel against the same values from the
+    solver's FP64 showdown terminal on a one-node tree (FP32 sums: 1e-5)."""
+    rng = np.random.default_rng(3)
+    meta = []
+    for _ in range(24):
+        board = [int(c) for c in rng.choice(52, 5, replace=False)]
+        live = ln._live_mask(board)
+        m = {"board": board}
+        for p in range(2):
+            w = rng.dirichlet(np.full(1326, rng.uniform(0.1, 1.0))) * live
+            m[f"range{p}"] = w / w.sum()
+        meta.append(m)
+    a = ln.checkdown_values(meta)
+    b = ln.checkdown_values_fp64(meta)
+    assert np.abs(a - b).max() <= 1e-5
