@@ -2,12 +2,12 @@
 // leaf network: C[M x N] = epilogue(A[M x K] * B[N x K]^T), A and B row-major
 // (K contiguous), FP32 accumulation in tensor memory.
 //
-// One 128 x 128 output tile per CTA of 192 threads:
-//   warp 0      one thread streams 128 x 64 tiles of A and B into a 4-stage
+// One 128 x 256 output tile per CTA of 192 threads:
+//   warp 0      one thread streams 128 x 64 tiles of A and 256 x 64 of B into a 4-stage
 //               shared-memory ring with 2-D TMA loads (128-byte swizzle),
 //               completing on the stage's "full" mbarrier;
-//   warp 1      allocates 128 TMEM columns; one thread issues
-//               tcgen05.mma (M=128, N=128, K=16, kind::f16, BF16 in, FP32
+//   warp 1      allocates 256 TMEM columns; one thread issues
+//               tcgen05.mma (M=128, N=256, K=16, kind::f16, BF16 in, FP32
 //               accumulate) four times per stage and commits each stage back
 //               to its "empty" mbarrier, then commits the accumulator;
 //   warps 2..5  read the accumulator with tcgen05.ld (warp w owns TMEM lanes
@@ -28,10 +28,10 @@
 namespace mtt {
 namespace gemm {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4, THREADS = 192;
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, THREADS = 192;
 constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // tiles (1024-aligned) + barriers
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TMEM_COLS = BN;   // one FP32 column per output column
 
 enum { F_RELU = 1, F_OUT_BF16 = 2, F_MASK = 4 };
 
@@ -203,13 +203,13 @@ static int encoder(PFN_cuTensorMapEncodeTiled_v12000* out) {
 }
 
 // 2-D map of a row-major bf16 matrix [rows x cols] with leading dimension ld,
-// box 64 (cols) x 128 (rows), 128-byte swizzle, zero fill outside.
-static int make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld) {
+// box 64 (cols) x box_rows (rows), 128-byte swizzle, zero fill outside.
+static int make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, int box_rows) {
     PFN_cuTensorMapEncodeTiled_v12000 enc;
     MTT_TRY(encoder(&enc));
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -224,8 +224,8 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     if (((uintptr_t)A & 15) || ((uintptr_t)B & 15)) return MTT_ERR_INVALID;
     if ((flags & F_MASK) && (!mask || ldm < N)) return MTT_ERR_INVALID;
     CUtensorMap ta, tb;
-    MTT_TRY(make_map(&ta, A, M, K, lda));
-    MTT_TRY(make_map(&tb, B, N, K, ldb));
+    MTT_TRY(make_map(&ta, A, M, K, lda, BM));
+    MTT_TRY(make_map(&tb, B, N, K, ldb, BN));
     MTT_TRY_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
     k_gemm_bf16<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, C, M, N, K, ldc, bias,

@@ -168,12 +168,15 @@ def checkdown_values(meta, device="cuda", stream=None):
     import torch
     n = len(meta)
     boards = np.asarray([m["board"] for m in meta], np.uint8).reshape(n, 5)
-    r = [np.zeros((n, 1326), np.float32), np.zeros((n, 1326), np.float32)]
-    for i, m in enumerate(meta):
-        live = _live_mask(m["board"])
-        for p in range(2):
-            v = np.asarray(m[f"range{p}"], np.float64) * live
-            r[p][i] = v / v.sum() if v.sum() > 0 else v
+    bm = np.bitwise_or.reduce(np.left_shift(np.uint64(1), boards.astype(np.uint64)), axis=1)      # [n]
+    cm = np.left_shift(np.uint64(1), _CARDS[:, 0].astype(np.uint64)) | \
+        np.left_shift(np.uint64(1), _CARDS[:, 1].astype(np.uint64))                               # [1326]
+    live = (bm[:, None] & cm[None, :]) == 0
+    r = []
+    for p in range(2):
+        v = np.stack([np.asarray(m[f"range{p}"], np.float64) for m in meta]) * live
+        tot = v.sum(axis=1, keepdims=True)
+        r.append(np.where(tot > 0, v / np.where(tot > 0, tot, 1.0), v).astype(np.float32))
     db = torch.from_numpy(boards).to(device)
     d0, d1 = torch.from_numpy(r[0]).to(device), torch.from_numpy(r[1]).to(device)
     out = torch.empty((n, OUT), dtype=torch.float32, device=device)
