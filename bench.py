@@ -28,6 +28,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "batched river solves/s at <=0.1% pot exploitability vs plain kernel; evals/s"
+# DRAM bytes (read + write) of one CFR iteration of the sweeps and terminals
+# (k_fwd x6, k_term x6, k_bwd x12) on the default workload (4096 subgames,
+# seed 2), from a one-pass ncu capture of dram__bytes_read.sum +
+# dram__bytes_write.sum over 26 complete iterations (min 13.167, max 13.179 GB);
+# the algorithmic bytes of the same iteration are 14.251 GB.
+TRAFFIC_PER_ITER = {"subgames": 4096, "seed": 2, "bytes": 13.175e9}
 
 
 def parse():
@@ -165,8 +171,10 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.subgames / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (seeded)",
-            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames x {args.iters} iters",
-                       "subgames": args.subgames, "iters": args.iters, "seed": args.seed},
+            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames, {args.iters} iterations "
+                                   f"+ FP64 exploitability, continued to <= {args.target * 100:g}% pot",
+                       "subgames_per_gpu": args.subgames, "iters": args.iters, "seed": args.seed,
+                       "parallelism": "host cores (the reference has no CPU path; the oracle restates its kernels)"},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -350,6 +358,8 @@ def run_b200(args, rank, world, local):
     solve_ms = k0.elapsed_time(k1)
     algo_bytes = info["iter_bytes"] * args.iters
     achieved = algo_bytes / (solve_ms * 1e-3) / 1e9
+    traffic = (TRAFFIC_PER_ITER["bytes"] if (args.subgames, args.seed) ==
+               (TRAFFIC_PER_ITER["subgames"], TRAFFIC_PER_ITER["seed"]) else None)
     peak, peak_kind = load_peaks()
     batch.close()
 
@@ -419,7 +429,9 @@ def run_b200(args, rank, world, local):
                              "sample": f"{n_plain} subgames solved one at a time, level launches, no graph"},
             "vs_plain": value / (1.0 / plain_s),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_unit": "DRAM bytes per CFR iteration (ncu capture of this workload)",
+                         "algorithmic_bytes_per_iter": int(info["iter_bytes"]),
                          "kernel": "CFR sweeps + terminals (k_fwd, k_term, k_bwd), no best response",
                          "peak_kind": peak_kind, "kernel_ms": solve_ms},
             "clocks": clocks,

@@ -378,7 +378,7 @@ __device__ __forceinline__ void bwd_sum_fixed(const float4* __restrict__ qc, flo
 
 // Forward sweep of one level: regret matching, children's reach and/or
 // strategy sums (kernel_forward_sweep, honest_multistreet_solver.cu:88-126).
-__global__ void __launch_bounds__(256, 3) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
+__global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __rest
 
 // Backward sweep of one level for the updated players: counterfactual values
 // and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
-__global__ void __launch_bounds__(256, 3) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+__global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
