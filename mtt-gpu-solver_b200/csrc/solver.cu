@@ -154,11 +154,12 @@ __device__ __forceinline__ TA cta_sum(TA v, TA* wb, int tid) {
 // Values of player q at a terminal against opponent reach `ro` (H_o entries),
 // written to out[0..Hp_q) (and out2), by one CTA of TT threads.  TI: stored
 // reach type, TA: arithmetic type of the scan and differences, TO: stored
-// value type.  The solver keeps reach and values in FP32 but scans in FP64:
-// win/tie/loss masses are differences of prefix sums, and a value that is
-// exactly zero (all of the opponent's remaining mass blocked by the hand's
-// cards) must come out as zero to the precision the regret-matching
-// threshold (1e-7) can see.  X: the CTA's shared scratch (term_scratch
+// value type.  The FP64 best response calls it with TA = double: win/tie/loss
+// masses are differences of prefix sums, and a value that is exactly zero
+// (all of the opponent's remaining mass blocked by the hand's cards) must
+// come out as zero to the precision the regret-matching threshold (1e-7)
+// can see.  The CFR sweeps use the fixed-point form below, which keeps that
+// property with 4-byte scan elements.  X: the CTA's shared scratch (term_scratch
 // elements), wb: NT/32 elements.  NT: threads of the CTA; the scan's chunks
 // depend on it, so each caller fixes it.
 template <typename TI, typename TA, typename TO, bool STAGED = false, int NT = TT>
@@ -273,6 +274,189 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         }
         out[h] = (TO)v;
         if (out2) out2[h] = (TO)v;
+    }
+    __syncthreads();
+}
+
+// Terminal values in 32-bit fixed point, for the CFR sweeps.  The opponent
+// reach at one terminal is scaled by a power of two 2^k chosen from its own
+// absolute sum S (S * 2^k < 2^29) and rounded to int32; every win / tie /
+// loss mass is then a difference of exact integer prefix sums.  Integer sums
+// do not depend on their order, so the scan's chunking cannot change a
+// result, and a mass that is exactly zero stays exactly zero (the property
+// the FP64 scan above exists for).  Every prefix sum over the three lists is
+// at most 3 * (2^29 + H/2) < 2^31 in magnitude; the value combinations below
+// are formed in unsigned (modular) arithmetic, exact because their true
+// values are below 2^31.  Each reach value is off by at most half a unit,
+// i.e. 2^-30 of S, far below FP32 resolution of S.  k is clamped to
+// [-126, 126] so 2^k and 2^-k are normal floats; the clamp can only bite
+// when S < 2^-97, where the values are below FP32 resolution of anything
+// else in the solve.
+//
+// Per terminal the CTA (1) sums |reach| over the opponent's hands, (2)
+// gathers, rounds and scans the opponent reach in scan order, each thread
+// holding a chunk of C consecutive positions in registers (C odd, so the
+// strided shared-memory accesses are conflict-free), (3) writes the
+// exclusive prefix, and (4) forms each hand's value from two integer masses:
+//   A = W + LE + same = 2 W + T   (twice the pot-share mass)
+//   B = Tt - C1 - C2 + same       (opponent mass not blocked by the hand)
+//   value = pot/2 * A - c * B     (= gain W + tie T + loss L)
+// Folds scan only the per-card lists (each opponent hand sits in two of
+// them, so their total is twice the opponent's mass) and use B.
+struct FxScale { float f, inv; };
+
+__device__ __forceinline__ FxScale fx_scale(float S) {
+    // S < 2^e with e from S's exponent field (denormal or zero S: e = -126)
+    const int E = (int)((__float_as_uint(S) >> 23) & 0xFFu);
+    const int e = E == 0 ? -126 : E - 126;
+    const int k = S > 0.f ? min(max(29 - e, -126), 126) : 0;
+    FxScale s;
+    s.f = __uint_as_float((uint32_t)(127 + k) << 23);
+    s.inv = __uint_as_float((uint32_t)(127 - k) << 23);
+    return s;
+}
+
+__device__ __forceinline__ int fx_round(float v, const FxScale& s) {
+    return __float2int_rn(__fmul_rn(v, s.f));   // a power-of-two product is exact
+}
+
+// Steps (2)-(3) for chunks of C positions.  idx: the opponent's hand index of
+// each scan position; X: N + 1 ints.  Returns the total.
+template <int NT, int C>
+__device__ __forceinline__ int fx_scan(const uint16_t* __restrict__ idx, const float* __restrict__ ro, int N,
+                                       const FxScale& fs, int* X, int* wi, int tid) {
+    const int lane = tid & 31, wid = tid >> 5;
+    const int s0 = min(tid * C, N);
+    int xv[C];
+    int loc = 0;
+    if (s0 + C <= N) {
+#pragma unroll
+        for (int j = 0; j < C; ++j) {
+            xv[j] = fx_round(ro[idx[s0 + j]], fs);
+            loc += xv[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < C; ++j) {
+            xv[j] = s0 + j < N ? fx_round(ro[idx[s0 + j]], fs) : 0;
+            loc += xv[j];
+        }
+    }
+    int inc = loc;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+        if (lane >= off) inc += t;
+    }
+    int run = inc - loc;
+    if (lane == 31) wi[wid] = inc;
+    __syncthreads();
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < NT / 32; ++k) {
+        const int w = wi[k];
+        if (k < wid) run += w;
+        total += w;
+    }
+    if (s0 + C <= N) {
+#pragma unroll
+        for (int j = 0; j < C; ++j) {
+            X[s0 + j] = run;
+            run += xv[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < C; ++j) {
+            if (s0 + j < N) X[s0 + j] = run;
+            run += xv[j];
+        }
+    }
+    if (tid == 0) X[N] = total;
+    __syncthreads();
+    return total;
+}
+
+// ro: the opponent reach staged in shared memory (16-byte aligned, zero past
+// Ho up to a multiple of 4); X: 3 * Ho + 8 ints; wf, wi: NT / 32 each.
+template <int NT>
+__device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, const float* __restrict__ ro,
+                                float* __restrict__ out, int* X, float* wf, int* wi, int semantics, int tid) {
+    static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
+    const int o = 1 - q;
+    const int Ho = ti.H[o], Hq = ti.H[q], Hpq = ti.Hp[q];
+    const uint16_t* seg = tv.seg[o];
+    const Entry* ent = tv.ent[q];
+    const bool fold = ti.type == MTT_NODE_FOLD;
+    const int lo = fold ? Ho : 0;            // folds scan only the per-card lists
+    const int N = 3 * Ho - lo;
+    const int cb = Ho - lo;                  // scan position of the per-card lists
+    const uint16_t* idx = tv.sorted[o] + lo; // [rank order (Ho) | per-card lists (2 Ho)], contiguous
+    // (1) absolute opponent mass
+    float part = 0.f;
+    const float4* ro4 = reinterpret_cast<const float4*>(ro);
+    for (int j = tid; j < (Ho >> 2); j += NT) {
+        const float4 r = ro4[j];
+        part += (fabsf(r.x) + fabsf(r.y)) + (fabsf(r.z) + fabsf(r.w));
+    }
+    if (tid < (Ho & 3)) part += fabsf(ro[(Ho & ~3) + tid]);
+    part = warp_sum(part);
+    if ((tid & 31) == 0) wf[tid >> 5] = part;
+    __syncthreads();
+    float S = 0.f;
+#pragma unroll
+    for (int k = 0; k < NT / 32; ++k) S += wf[k];
+    const FxScale fs = fx_scale(S);
+    // (2)-(3)
+    const int C = ((N + NT - 1) / NT) | 1;
+    int total;
+    switch (C) {
+        case 1: total = fx_scan<NT, 1>(idx, ro, N, fs, X, wi, tid); break;
+        case 3: total = fx_scan<NT, 3>(idx, ro, N, fs, X, wi, tid); break;
+        case 5: total = fx_scan<NT, 5>(idx, ro, N, fs, X, wi, tid); break;
+        case 7: total = fx_scan<NT, 7>(idx, ro, N, fs, X, wi, tid); break;
+        case 9: total = fx_scan<NT, 9>(idx, ro, N, fs, X, wi, tid); break;
+        case 11: total = fx_scan<NT, 11>(idx, ro, N, fs, X, wi, tid); break;
+        case 13: total = fx_scan<NT, 13>(idx, ro, N, fs, X, wi, tid); break;
+        case 15: total = fx_scan<NT, 15>(idx, ro, N, fs, X, wi, tid); break;
+        default: total = fx_scan<NT, 17>(idx, ro, N, fs, X, wi, tid); break;
+    }
+    // (4)
+    const unsigned Tt = (unsigned)(fold ? total >> 1 : X[Ho]);   // total is even: exact halving
+    const float cq = ti.c[q], pot = ti.pot;
+    const float ga = __fmul_rn(__fmul_rn(0.5f, pot), fs.inv), gc = __fmul_rn(cq, fs.inv);
+    const float gp = __fmul_rn((q == ((ti.wmask == 1) ? 0 : 1)) ? pot - cq : -cq, fs.inv);
+    for (int h = tid; h < Hpq; h += NT) {
+        float v = 0.f;
+        if (h < Hq) {
+            const Entry et = ent[h];
+            if (et.lt != 0xFFFFu) {
+                if (fold && semantics) {
+                    v = gp * (float)(int)Tt;
+                } else {
+                    const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
+                    const int s1c = cb + seg[et.c1], s2c = cb + seg[et.c2];
+                    const unsigned b1 = (unsigned)X[s1c], b2 = (unsigned)X[s2c];
+                    const unsigned B = Tt - ((unsigned)X[cb + seg[et.c1 + 1]] - b1) -
+                                       ((unsigned)X[cb + seg[et.c2 + 1]] - b2) + ps;
+                    if (fold) {
+                        v = gp * (float)(int)B;
+                    } else {
+                        const unsigned A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] -
+                                           (unsigned)X[s1c + et.lec1] - (unsigned)X[s2c + et.ltc2] -
+                                           (unsigned)X[s2c + et.lec2] + 2u * (b1 + b2) + ps;
+                        if (!semantics) {
+                            v = ga * (float)(int)A - gc * (float)(int)B;
+                        } else {
+                            // blocked pairs count as P0 losses (honest:182-187): B = Tt,
+                            // and player 1's pot share is 2 Lr + T = 2 Tt - A
+                            const unsigned Aq = q == 0 ? A : 2u * Tt - A;
+                            v = ga * (float)(int)Aq - gc * (float)(int)Tt;
+                        }
+                    }
+                }
+            }
+        }
+        out[h] = v;
     }
     __syncthreads();
 }
@@ -477,27 +661,27 @@ __host__ __device__ inline int tg_table_bytes(int H0, int H1, int upd) {
 __host__ __device__ inline int tg_reach_bytes(int Hp0, int Hp1, int upd) {
     return upd == 3 ? 4 * (Hp0 + Hp1) : 4 * (upd == 1 ? Hp1 : Hp0);
 }
-__host__ __device__ inline int tg_scan_doubles(int H0, int H1, int upd) {
+__host__ __device__ inline int tg_scan_ints(int H0, int H1, int upd) {
     int m = 0;
     for (int q = 0; q < 2; ++q) {
         if (!((upd >> q) & 1)) continue;
         const int Ho = q ? H0 : H1;
-        const int need = (3 * Ho + 8) > (2 * Ho + 64) ? (3 * Ho + 8) : (2 * Ho + 64);
-        m = need > m ? need : m;
+        m = 3 * Ho + 8 > m ? 3 * Ho + 8 : m;
     }
     return m;
 }
 __host__ __device__ inline int tg_smem_bytes(int H0, int H1, int Hp0, int Hp1, int upd) {
-    return tg_table_bytes(H0, H1, upd) + 2 * tg_reach_bytes(Hp0, Hp1, upd) + 8 * tg_scan_doubles(H0, H1, upd) + 16;
+    return tg_table_bytes(H0, H1, upd) + 2 * tg_reach_bytes(Hp0, Hp1, upd) + 4 * tg_scan_ints(H0, H1, upd) + 16;
 }
 
 // Terminal values of the updated players (kernel_evaluate_terminals,
 // honest_multistreet_solver.cu:128-196), one terminal group per CTA.
-__global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __restrict__ groups,
+__global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __restrict__ groups,
                                              const TermItem* __restrict__ items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s
-    __shared__ double wb[TG / 32];
+    __shared__ float wf[TG / 32];
+    __shared__ int wi[TG / 32];
     const int gi = blockIdx.x, tid = threadIdx.x;
     if (gi >= n) return;
     const TermGroup g = groups[gi];
@@ -508,7 +692,7 @@ __global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __rest
     uint8_t* T = smem;
     float* Rst0 = reinterpret_cast<float*>(smem + tb);
     float* Rst1 = reinterpret_cast<float*>(smem + tb + rbytes);
-    double* X = reinterpret_cast<double*>(smem + tb + 2 * rbytes);   // tb, rbytes: multiples of 16
+    int* X = reinterpret_cast<int*>(smem + tb + 2 * rbytes);   // tb, rbytes: multiples of 16
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -585,8 +769,7 @@ __global__ void __launch_bounds__(TG) k_term(SolveDev a, const TermGroup* __rest
             if (!((upd >> q) & 1)) continue;
             // opponent reach: player 1's part follows player 0's in a two-direction stage
             const float* ro = both ? (q == 0 ? st + g.Hp0 : st) : st;
-            cta_terminal<float, double, float, true, TG>(ti, tv, q, ro, a.arena + it.out[q], nullptr, X, wb,
-                                                         a.semantics, tid);
+            cta_terminal_fx<TG>(ti, tv, q, ro, a.arena + it.out[q], X, wf, wi, a.semantics, tid);
         }
     }
 }
