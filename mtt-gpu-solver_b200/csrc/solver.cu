@@ -53,6 +53,12 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
 __device__ __forceinline__ float4 mul4(float4 a, float4 b) {
     return make_float4(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z), __fmul_rn(a.w, b.w));
 }
+// Starts a fetch of the line holding p into L2 (no register is written, so
+// every row of a work item can be requested before its first use).
+__device__ __forceinline__ void pf_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
 __device__ __forceinline__ float4 max04(float4 a) {
     return make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
 }
@@ -606,6 +612,8 @@ __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __res
     }
     const float invA = __fdiv_rn(1.0f, (float)A);
     float w_lin = 0.f, dstr = 0.f;
+    if (ds && it.g0 + lane < H4)
+        for (int k = 0; k < A; ++k) pf_l2(Sb + (size_t)k * H4 + it.g0 + lane);
     if (ds) {
         const float4 tb = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (*a.iter - 1));
         w_lin = tb.x;
@@ -827,6 +835,10 @@ __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __res
     float dpos = 0.f, dneg = 0.f, w_lin = 0.f, dstr = 0.f;
     const bool dcfr = a.algo == MTT_ALGO_DCFR;
     const bool ds = it.flags & BI_SUMS;
+    for (int k = 0; k < A; ++k) {
+        pf_l2(qc + (size_t)k * HS4 + g);
+        if (ds) pf_l2(reinterpret_cast<const float4*>(a.S + it.rows) + (size_t)k * H4 + g);
+    }
     if (dcfr || ds) {
         const float4 tb = *reinterpret_cast<const float4*>(a.iter_tab + 4 * (*a.iter - 1));
         dpos = tb.y;
