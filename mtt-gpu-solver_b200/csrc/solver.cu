@@ -382,22 +382,10 @@ __device__ __forceinline__ int fx_scan(const uint16_t* __restrict__ idx, const f
     return total;
 }
 
-// ro: the opponent reach staged in shared memory (16-byte aligned, zero past
-// Ho up to a multiple of 4); X: 3 * Ho + 8 ints; wf, wi: NT / 32 each.
+// This thread's share of the opponent's absolute mass sum |ro[j]|, j < Ho,
+// reduced over its warp (valid in lane 0).  ro: 16-byte aligned.
 template <int NT>
-__device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, const float* __restrict__ ro,
-                                float* __restrict__ out, int* X, float* wf, int* wi, int semantics, int tid) {
-    static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
-    const int o = 1 - q;
-    const int Ho = ti.H[o], Hq = ti.H[q], Hpq = ti.Hp[q];
-    const uint16_t* seg = tv.seg[o];
-    const Entry* ent = tv.ent[q];
-    const bool fold = ti.type == MTT_NODE_FOLD;
-    const int lo = fold ? Ho : 0;            // folds scan only the per-card lists
-    const int N = 3 * Ho - lo;
-    const int cb = Ho - lo;                  // scan position of the per-card lists
-    const uint16_t* idx = tv.sorted[o] + lo; // [rank order (Ho) | per-card lists (2 Ho)], contiguous
-    // (1) absolute opponent mass
+__device__ __forceinline__ float fx_abs_part(const float* __restrict__ ro, int Ho, int tid) {
     float part = 0.f;
     const float4* ro4 = reinterpret_cast<const float4*>(ro);
     for (int j = tid; j < (Ho >> 2); j += NT) {
@@ -405,14 +393,65 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, co
         part += (fabsf(r.x) + fabsf(r.y)) + (fabsf(r.z) + fabsf(r.w));
     }
     if (tid < (Ho & 3)) part += fabsf(ro[(Ho & ~3) + tid]);
-    part = warp_sum(part);
-    if ((tid & 31) == 0) wf[tid >> 5] = part;
-    __syncthreads();
-    float S = 0.f;
-#pragma unroll
-    for (int k = 0; k < NT / 32; ++k) S += wf[k];
+    return warp_sum(part);
+}
+
+// Per-card quantities of one scan, 52 entries each: the scan position of the
+// card's list, twice the prefix at that position, and the list's mass.
+struct FxCards {
+    int pos[52];
+    int b2[52];
+    int mass[52];
+};
+
+// Value of hand h of player q from the scanned prefix sums (step 4).
+struct FxEval {
+    const Entry* ent;
+    const FxCards* cd;
+    const int* X;
+    const float* ro;
+    FxScale fs;
+    unsigned Tt;
+    float ga, gc, gp;
+    int Hq, q, semantics;
+    bool fold;
+
+    __device__ __forceinline__ float operator()(int h) const {
+        if (h >= Hq) return 0.f;
+        const Entry et = ent[h];
+        if (et.lt == 0xFFFFu) return 0.f;
+        if (fold && semantics) return gp * (float)(int)Tt;
+        const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
+        const unsigned B = Tt - (unsigned)cd->mass[et.c1] - (unsigned)cd->mass[et.c2] + ps;
+        if (fold) return gp * (float)(int)B;
+        const int s1c = cd->pos[et.c1], s2c = cd->pos[et.c2];
+        const unsigned A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] -
+                           (unsigned)X[s1c + et.lec1] - (unsigned)X[s2c + et.ltc2] - (unsigned)X[s2c + et.lec2] +
+                           (unsigned)cd->b2[et.c1] + (unsigned)cd->b2[et.c2] + ps;
+        if (!semantics) return ga * (float)(int)A - gc * (float)(int)B;
+        // blocked pairs count as P0 losses (honest:182-187): B = Tt, and
+        // player 1's pot share is 2 Lr + T = 2 Tt - A
+        const unsigned Aq = q == 0 ? A : 2u * Tt - A;
+        return ga * (float)(int)Aq - gc * (float)(int)Tt;
+    }
+};
+
+// Steps (2)-(4) for player q against the opponent reach ro (staged in shared
+// memory, 16-byte aligned, zero past Ho up to a multiple of 4), whose
+// absolute mass S the caller has reduced.  X: 3 * Ho + 8 ints; wi: NT / 32.
+// Ends without a barrier: the caller's next barrier must come before X or ro
+// is written again.
+template <int NT>
+__device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, const float* __restrict__ ro, float S,
+                                float* __restrict__ out, int* X, int* wi, FxCards* cd, int semantics, int tid) {
+    static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
+    const int o = 1 - q;
+    const int Ho = ti.H[o], Hpq = ti.Hp[q];
+    const bool fold = ti.type == MTT_NODE_FOLD;
+    const int lo = fold ? Ho : 0;            // folds scan only the per-card lists
+    const int N = 3 * Ho - lo;
+    const uint16_t* idx = tv.sorted[o] + lo; // [rank order (Ho) | per-card lists (2 Ho)], contiguous
     const FxScale fs = fx_scale(S);
-    // (2)-(3)
     const int C = ((N + NT - 1) / NT) | 1;
     int total;
     switch (C) {
@@ -426,45 +465,31 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, co
         case 15: total = fx_scan<NT, 15>(idx, ro, N, fs, X, wi, tid); break;
         default: total = fx_scan<NT, 17>(idx, ro, N, fs, X, wi, tid); break;
     }
-    // (4)
-    const unsigned Tt = (unsigned)(fold ? total >> 1 : X[Ho]);   // total is even: exact halving
-    const float cq = ti.c[q], pot = ti.pot;
-    const float ga = __fmul_rn(__fmul_rn(0.5f, pot), fs.inv), gc = __fmul_rn(cq, fs.inv);
-    const float gp = __fmul_rn((q == ((ti.wmask == 1) ? 0 : 1)) ? pot - cq : -cq, fs.inv);
-    for (int h = tid; h < Hpq; h += NT) {
-        float v = 0.f;
-        if (h < Hq) {
-            const Entry et = ent[h];
-            if (et.lt != 0xFFFFu) {
-                if (fold && semantics) {
-                    v = gp * (float)(int)Tt;
-                } else {
-                    const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
-                    const int s1c = cb + seg[et.c1], s2c = cb + seg[et.c2];
-                    const unsigned b1 = (unsigned)X[s1c], b2 = (unsigned)X[s2c];
-                    const unsigned B = Tt - ((unsigned)X[cb + seg[et.c1 + 1]] - b1) -
-                                       ((unsigned)X[cb + seg[et.c2 + 1]] - b2) + ps;
-                    if (fold) {
-                        v = gp * (float)(int)B;
-                    } else {
-                        const unsigned A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] -
-                                           (unsigned)X[s1c + et.lec1] - (unsigned)X[s2c + et.ltc2] -
-                                           (unsigned)X[s2c + et.lec2] + 2u * (b1 + b2) + ps;
-                        if (!semantics) {
-                            v = ga * (float)(int)A - gc * (float)(int)B;
-                        } else {
-                            // blocked pairs count as P0 losses (honest:182-187): B = Tt,
-                            // and player 1's pot share is 2 Lr + T = 2 Tt - A
-                            const unsigned Aq = q == 0 ? A : 2u * Tt - A;
-                            v = ga * (float)(int)Aq - gc * (float)(int)Tt;
-                        }
-                    }
-                }
-            }
-        }
-        out[h] = v;
+    const int cb = Ho - lo;                  // scan position of the per-card lists
+    if (tid < 52) {
+        const uint16_t* seg = tv.seg[o];
+        const int p = cb + seg[tid];
+        const int b = X[p];
+        cd->pos[tid] = p;
+        cd->b2[tid] = (int)(2u * (unsigned)b);
+        cd->mass[tid] = X[cb + seg[tid + 1]] - b;
     }
     __syncthreads();
+    FxEval ev;
+    ev.ent = tv.ent[q]; ev.cd = cd; ev.X = X; ev.ro = ro; ev.fs = fs;
+    ev.Tt = (unsigned)(fold ? total >> 1 : X[Ho]);   // total is even: exact halving
+    const float cq = ti.c[q], pot = ti.pot;
+    ev.ga = __fmul_rn(__fmul_rn(0.5f, pot), fs.inv);
+    ev.gc = __fmul_rn(cq, fs.inv);
+    ev.gp = __fmul_rn((q == ((ti.wmask == 1) ? 0 : 1)) ? pot - cq : -cq, fs.inv);
+    ev.Hq = ti.H[q]; ev.q = q; ev.semantics = semantics; ev.fold = fold;
+    // two hands per step: their dependent shared-memory chains overlap
+    for (int h = tid; h < Hpq; h += 2 * NT) {
+        const float v0 = ev(h);
+        const float v1 = ev(h + NT);
+        out[h] = v0;
+        if (h + NT < Hpq) out[h + NT] = v1;
+    }
 }
 
 // ------------------------------------------------------------- solve kernels
@@ -688,8 +713,9 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
                                              const TermItem* __restrict__ items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s
-    __shared__ float wf[TG / 32];
+    __shared__ float wf[2][2][TG / 32];   // [terminal parity][updated player][warp]
     __shared__ int wi[TG / 32];
+    __shared__ FxCards cards;
     const int gi = blockIdx.x, tid = threadIdx.x;
     if (gi >= n) return;
     const TermGroup g = groups[gi];
@@ -756,18 +782,32 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
     }
     TermInfo ti;
     ti.H[0] = g.H0; ti.H[1] = g.H1; ti.Hp[0] = g.Hp0; ti.Hp[1] = g.Hp1;
-    uint32_t parity = 0u;   // bit s: phase of stage s
+    // opponent reach of player q inside a stage: player 1's part follows
+    // player 0's in a two-direction stage
+    auto opp = [&](const float* st, int q) -> const float* { return both ? (q == 0 ? st + g.Hp0 : st) : st; };
+    // absolute opponent masses of the terminal staged in st, per updated
+    // player, into wf[buf]; read after the next barrier
+    auto mass_parts = [&](const float* st, int buf) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (!((upd >> q) & 1)) continue;
+            const float p = fx_abs_part<TG>(opp(st, q), q ? g.H0 : g.H1, tid);
+            if ((tid & 31) == 0) wf[buf][q][tid >> 5] = p;
+        }
+    };
+    uint32_t parity = 1u;   // bit s: phase of stage s's next wait (stage 0's first is done below)
+    {
+        const bool ok = mbar_wait_bounded(&bar[1], 0u);
+        if (ok) mass_parts(Rst0, 0);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(a.err, 1);
+            return;
+        }
+    }
     for (int t = 0; t < g.count; ++t) {
         const int s = t & 1;
         // stage s ^ 1 was last read by terminal t - 1, which ended on a barrier
         if (tid == 0 && t + 1 < g.count) issue_reach(t + 1, s ^ 1);
-        const bool ok = mbar_wait_bounded(&bar[1 + s], (parity >> s) & 1u);
-        parity ^= 1u << s;
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(a.err, 1);
-            if (t + 1 < g.count) (void)mbar_wait_bounded(&bar[2 - s], (parity >> (s ^ 1)) & 1u);
-            return;
-        }
         const TermItem& it = items[g.first + t];
         ti.pot = it.pot; ti.c[0] = it.c0; ti.c[1] = it.c1;
         ti.type = it.type_wmask & 0xFF; ti.wmask = (it.type_wmask >> 8) & 0xFF;
@@ -775,9 +815,22 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             if (!((upd >> q) & 1)) continue;
-            // opponent reach: player 1's part follows player 0's in a two-direction stage
-            const float* ro = both ? (q == 0 ? st + g.Hp0 : st) : st;
-            cta_terminal_fx<TG>(ti, tv, q, ro, a.arena + it.out[q], X, wf, wi, a.semantics, tid);
+            float S = 0.f;
+#pragma unroll
+            for (int k = 0; k < TG / 32; ++k) S += wf[s][q][k];
+            if (both && q == 1) __syncthreads();   // player 0's values have been read out of X
+            cta_terminal_fx<TG>(ti, tv, q, opp(st, q), S, a.arena + it.out[q], X, wi, &cards, a.semantics, tid);
+        }
+        // terminal t + 1's reach and masses; the barrier also ends terminal t
+        bool ok = true;
+        if (t + 1 < g.count) {
+            ok = mbar_wait_bounded(&bar[2 - s], (parity >> (s ^ 1)) & 1u);
+            parity ^= 1u << (s ^ 1);
+            if (ok) mass_parts(s ? Rst0 : Rst1, s ^ 1);
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(a.err, 1);
+            return;
         }
     }
 }
