@@ -361,6 +361,18 @@ def run_b200(args, rank, world, local):
     traffic = (TRAFFIC_PER_ITER["bytes"] if (args.subgames, args.seed) ==
                (TRAFFIC_PER_ITER["subgames"], TRAFFIC_PER_ITER["seed"]) else None)
     peak, peak_kind = load_peaks()
+    # per kernel class: CUDA events around each class in every pass (level
+    # launches without the graph), compulsory bytes from the work lists
+    kp = batch.kernel_profile(ps, iters=min(args.iters, 10))
+    kernels = {}
+    for k, v in kp.items():
+        gbs = v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] > 0 else 0.0
+        kernels[k] = {"ms_per_iter": v["ms"], "compulsory_bytes_per_iter": int(v["bytes"]), "gbs": gbs,
+                      "frac": gbs / peak}
+    sw_b = kp["k_fwd"]["bytes"] + kp["k_bwd"]["bytes"]
+    sw_ms = kp["k_fwd"]["ms"] + kp["k_bwd"]["ms"]
+    kernels["sweeps"] = {"kernels": "k_fwd + k_bwd", "gbs": sw_b / (sw_ms * 1e-3) / 1e9,
+                         "frac": sw_b / (sw_ms * 1e-3) / 1e9 / peak}
     batch.close()
 
     # end to end through the public API from host buffers
@@ -433,7 +445,7 @@ def run_b200(args, rank, world, local):
                          "traffic_unit": "DRAM bytes per CFR iteration (ncu capture of this workload)",
                          "algorithmic_bytes_per_iter": int(info["iter_bytes"]),
                          "kernel": "CFR sweeps + terminals (k_fwd, k_term, k_bwd), no best response",
-                         "peak_kind": peak_kind, "kernel_ms": solve_ms},
+                         "peak_kind": peak_kind, "kernel_ms": solve_ms, "per_kernel": kernels},
             "clocks": clocks,
             "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(args.subgames * 6 * 8)},

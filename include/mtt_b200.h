@@ -288,6 +288,14 @@ int mtt_batch_check(mtt_batch* b, void* stream);
 /* Kernels launched for this batch since it was created; a graph replay counts
  * every kernel node it runs. No reference counterpart (instrumentation). */
 int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
+/* Runs `iters` CFR iterations (no best response, no graph) with a CUDA event
+ * around each kernel class of every pass and returns, per iteration,
+ * h_ms[3] = device time and h_bytes[3] = compulsory bytes (every element a
+ * work item reads or writes, counted once) of {forward sweeps, terminal
+ * launches, backward sweeps}.  Restarts the batch's solve state.  Blocks.
+ * No reference counterpart (instrumentation). */
+int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
+                             double* h_bytes, void* stream);
 /* Pick the CTA size by timing a few iterations of each candidate on this
  * batch; *threads receives the choice (also used when params.threads == 0). */
 int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads);

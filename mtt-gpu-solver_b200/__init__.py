@@ -329,6 +329,17 @@ class RiverBatch:
         check("mtt_batch_launch_count", lib().mtt_batch_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    def kernel_profile(self, params, iters=10, stream=None):
+        """Per-iteration device time (ms) and compulsory bytes of the forward
+        sweeps, terminal launches and backward sweeps, timed with CUDA events
+        around each kernel class over `iters` iterations (restarts the solve)."""
+        ms = np.zeros(3, dtype=np.float64)
+        by = np.zeros(3, dtype=np.float64)
+        check("mtt_batch_kernel_profile", lib().mtt_batch_kernel_profile(
+            self._h, ctypes.byref(params), int(iters), ms.ctypes.data, by.ctypes.data, _stream(stream)))
+        return {k: {"ms": float(ms[i]), "bytes": float(by[i])}
+                for i, k in enumerate(("k_fwd", "k_term", "k_bwd"))}
+
     def autotune(self, params, stream=None):
         t = ctypes.c_int32()
         check("mtt_batch_autotune", lib().mtt_batch_autotune(self._h, ctypes.byref(params), _stream(stream),

@@ -113,6 +113,7 @@ def lib():
         "mtt_batch_info": ([vp, vp, vp], ctypes.c_int),
         "mtt_batch_root_values": ([vp, i32, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_launch_count": ([vp, vp], ctypes.c_int),
+        "mtt_batch_kernel_profile": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
         "mtt_batch_layout": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_ev_grad": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_check": ([vp, vp], ctypes.c_int),

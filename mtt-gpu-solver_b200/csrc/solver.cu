@@ -1723,7 +1723,114 @@ static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, b
     }
     return MTT_OK;
 }
+// Compulsory bytes of one work item: every element it reads or writes,
+// counted once (the second read of a regret row hits L1).  g: float4 groups
+// the item's warp covers.
+static double fwd_item_bytes(const FwdItem& it) {
+    const double g = (double)std::min(32, it.h4 - it.g0), row = 16.0 * g, A = it.na;
+    if (it.flags & FI_CHANCE) return row * (1.0 + A) + 8.0 * g;       // reach, children, hand cards
+    return row * (1.0 + A + ((it.flags & FI_REACH) ? A : 0.0) + ((it.flags & FI_SUMS) ? 2.0 * A : 0.0));
+}
+static double bwd_item_bytes(const BwdItem& it) {
+    const double g = (double)std::min(32, it.h4 - it.g0), row = 16.0 * g, A = it.na;
+    if (it.flags & BI_CHANCE) return row * (A + 1.0) + 8.0 * g;       // children, value, hand cards
+    if (!(it.flags & BI_UPDATE)) return row * (A + 1.0);
+    // regret rows read and written, children read, value written; sums: reach and S rows
+    return row * (3.0 * A + 1.0 + ((it.flags & BI_SUMS) ? 1.0 + 2.0 * A : 0.0));
+}
+// Terminal launch for the updated players `upd`: each group's table blocks,
+// then per terminal the opponent reach read and the values written.
+static double term_launch_bytes(const ListSet& L, const std::vector<TermGroup>& gr, const std::vector<TermItem>& ti,
+                                int upd) {
+    (void)L;
+    double b = 0.0;
+    for (const TermGroup& g : gr) {
+        b += (double)tg_table_bytes(g.H0, g.H1, upd);
+        for (int t = g.first; t < g.first + g.count; ++t)
+            for (int q = 0; q < 2; ++q)
+                if ((upd >> q) & 1) b += 4.0 * ((double)ti[t].Hp[1 - q] + (double)ti[t].Hp[q]);
+    }
+    return b;
+}
 }  // namespace mtt
+
+extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
+                                        double* h_bytes, void* stream) {
+    using namespace mtt;
+    if (!b || !h_ms || !h_bytes || iters <= 0) return MTT_ERR_INVALID;
+    MTT_TRY(check_params(prm));
+    const mtt_solve_params& p = *prm;
+    cudaStream_t st = as_stream(stream);
+    const int threads = p.threads ? p.threads : (b->tuned_threads ? b->tuned_threads : 256);
+    const ListSet& L = b->full;
+    MTT_TRY(set_smem_attrs(b, L));
+    MTT_TRY(fill_iter_table(b, p, iters, st));
+    const SolveDev a = dev_args(b, p);
+    // per-iteration compulsory bytes of each kernel class, from the host lists
+    const HostLists& HL = b->host;
+    double bf = 0.0, bb = 0.0, bt = 0.0;
+    std::vector<TermGroup> gr(L.tb_start.empty() ? 0 : (size_t)(L.tb_start.back() + L.tb_count.back()));
+    if (!gr.empty())
+        MTT_TRY_CUDA(cudaMemcpy(gr.data(), L.tgroups, sizeof(TermGroup) * gr.size(), cudaMemcpyDeviceToHost));
+    if (p.alternate) {
+        for (int u = 0; u < 2; ++u) {
+            for (const auto& lv : HL.fal[u]) for (const FwdItem& it : lv) bf += fwd_item_bytes(it);
+            for (const auto& lv : HL.bal[u]) for (const BwdItem& it : lv) bb += bwd_item_bytes(it);
+            bt += term_launch_bytes(L, gr, HL.titems, 1 << u);
+        }
+    } else {
+        for (const auto& lv : HL.fsim) for (const FwdItem& it : lv) bf += fwd_item_bytes(it);
+        for (const auto& lv : HL.bsim) for (const BwdItem& it : lv) bb += bwd_item_bytes(it);
+        bt += term_launch_bytes(L, gr, HL.titems, 3);
+    }
+    h_bytes[0] = bf; h_bytes[1] = bt; h_bytes[2] = bb;
+    k_init<<<b->n, 256, 0, st>>>(a, b->n);
+    MTT_CHECK_LAUNCH();
+    ++b->launches;
+    MTT_TRY(launch_levels_fwd(b, a, L.f_init, threads, st));
+    // one event before and after each kernel class of every pass
+    const int passes = p.alternate ? 2 : 1, ne = 6 * passes;
+    std::vector<cudaEvent_t> ev(ne, nullptr);
+    int s = MTT_OK;
+    for (int i = 0; i < ne && !s; ++i) s = cuda_status(cudaEventCreate(&ev[i]));
+    double ms[3] = {0.0, 0.0, 0.0};
+    for (int t = 0; t < iters && !s; ++t) {
+        for (int u = 0; u < passes && !s; ++u) {
+            cudaEvent_t* e = ev.data() + 6 * u;
+            const LevelLists<FwdItem>& F = p.alternate ? L.f_alt[u] : L.f_sim;
+            const LevelLists<BwdItem>& B = p.alternate ? L.b_alt[u] : L.b_sim;
+            s = cuda_status(cudaEventRecord(e[0], st));
+            if (!s) s = launch_levels_fwd(b, a, F, threads, st);
+            if (!s) s = cuda_status(cudaEventRecord(e[1], st));
+            if (!s) s = cuda_status(cudaEventRecord(e[2], st));
+            if (!s) s = launch_term(b, L, a, p.alternate ? 1 << u : 3, st);
+            if (!s) s = cuda_status(cudaEventRecord(e[3], st));
+            if (!s) s = cuda_status(cudaEventRecord(e[4], st));
+            if (!s) s = launch_levels_bwd(b, a, B, threads, st);
+            if (!s) s = cuda_status(cudaEventRecord(e[5], st));
+        }
+        if (!s) {
+            k_next_iter<<<1, 32, 0, st>>>(a);
+            s = cuda_status(cudaGetLastError());
+            ++b->launches;
+        }
+        if (!s) s = cuda_status(cudaStreamSynchronize(st));
+        for (int u = 0; u < passes && !s; ++u) {
+            for (int k = 0; k < 3 && !s; ++k) {
+                float x = 0.f;
+                s = cuda_status(cudaEventElapsedTime(&x, ev[6 * u + 2 * k], ev[6 * u + 2 * k + 1]));
+                ms[k] += x;
+            }
+        }
+    }
+    for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+    if (s) return s;
+    std::fill(b->iters_done.begin(), b->iters_done.end(), iters);
+    for (int k = 0; k < 3; ++k) h_ms[k] = ms[k] / iters;
+    int err = 0;
+    MTT_TRY_CUDA(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return err ? MTT_ERR_TIMEOUT : MTT_OK;
+}
 
 extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** out) {
     if (!subs || n <= 0 || !out) return MTT_ERR_INVALID;

@@ -185,3 +185,20 @@ def test_config1_full_solve(mtt, wl, cuda):
     b.close()
     assert np.isfinite(r).all()
     assert r[5] < e50 and r[5] < 5e-3, (e50, r[5])
+
+
+def test_kernel_profile_reports_each_kernel_class(mtt, wl, cuda):
+    subs = wl.river_batch(n=8, seed=21, min_support=60, max_support=200, max_sizes=2)
+    b = mtt.RiverBatch(subs)
+    p = mtt.solve_params(iters=3, alternate=True, threads=128)
+    prof = b.kernel_profile(p, iters=3)
+    for k in ("k_fwd", "k_term", "k_bwd"):
+        assert prof[k]["ms"] > 0.0 and prof[k]["bytes"] > 0.0, (k, prof[k])
+    # the profiled iterations are ordinary ones: a solve afterwards is unaffected
+    b.solve(p)
+    r1 = b.results()
+    b2 = mtt.RiverBatch(subs)
+    b2.solve(p)
+    assert np.array_equal(r1, b2.results())
+    b.close()
+    b2.close()
