@@ -404,7 +404,20 @@ struct FxCards {
     int mass[52];
 };
 
-// Value of hand h of player q from the scanned prefix sums (step 4).
+// One terminal of a unit: where its values go and its payoff scalars.
+struct FxItem {
+    float* out;
+    float pot, c0, c1;
+    int type, wmask;
+};
+
+// The two integer masses of hand h (step 4); live = false for padding and
+// hands blocked by the dealt card.
+struct FxHand {
+    unsigned A, B;
+    bool live;
+};
+
 struct FxEval {
     const Entry* ent;
     const FxCards* cd;
@@ -412,43 +425,55 @@ struct FxEval {
     const float* ro;
     FxScale fs;
     unsigned Tt;
-    float ga, gc, gp;
     int Hq, q, semantics;
-    bool fold;
+    bool need_A;
 
-    __device__ __forceinline__ float operator()(int h) const {
-        if (h >= Hq) return 0.f;
+    __device__ __forceinline__ FxHand hand(int h) const {
+        FxHand x{0u, 0u, false};
+        if (h >= Hq) return x;
         const Entry et = ent[h];
-        if (et.lt == 0xFFFFu) return 0.f;
-        if (fold && semantics) return gp * (float)(int)Tt;
+        if (et.lt == 0xFFFFu) return x;
+        x.live = true;
         const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
-        const unsigned B = Tt - (unsigned)cd->mass[et.c1] - (unsigned)cd->mass[et.c2] + ps;
-        if (fold) return gp * (float)(int)B;
-        const int s1c = cd->pos[et.c1], s2c = cd->pos[et.c2];
-        const unsigned A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] -
-                           (unsigned)X[s1c + et.lec1] - (unsigned)X[s2c + et.ltc2] - (unsigned)X[s2c + et.lec2] +
-                           (unsigned)cd->b2[et.c1] + (unsigned)cd->b2[et.c2] + ps;
-        if (!semantics) return ga * (float)(int)A - gc * (float)(int)B;
+        x.B = Tt - (unsigned)cd->mass[et.c1] - (unsigned)cd->mass[et.c2] + ps;
+        if (need_A) {
+            const int s1c = cd->pos[et.c1], s2c = cd->pos[et.c2];
+            x.A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] - (unsigned)X[s1c + et.lec1] -
+                  (unsigned)X[s2c + et.ltc2] - (unsigned)X[s2c + et.lec2] + (unsigned)cd->b2[et.c1] +
+                  (unsigned)cd->b2[et.c2] + ps;
+        }
+        return x;
+    }
+
+    // ga = pot/2 * 2^-k, gc = c * 2^-k, gp = fold payoff * 2^-k
+    __device__ __forceinline__ float value(const FxHand& x, bool fold, float ga, float gc, float gp) const {
+        if (!x.live) return 0.f;
+        if (fold) return gp * (float)(int)(semantics ? Tt : x.B);
+        if (!semantics) return ga * (float)(int)x.A - gc * (float)(int)x.B;
         // blocked pairs count as P0 losses (honest:182-187): B = Tt, and
         // player 1's pot share is 2 Lr + T = 2 Tt - A
-        const unsigned Aq = q == 0 ? A : 2u * Tt - A;
+        const unsigned Aq = q == 0 ? x.A : 2u * Tt - x.A;
         return ga * (float)(int)Aq - gc * (float)(int)Tt;
     }
 };
 
-// Steps (2)-(4) for player q against the opponent reach ro (staged in shared
-// memory, 16-byte aligned, zero past Ho up to a multiple of 4), whose
-// absolute mass S the caller has reduced.  X: 3 * Ho + 8 ints; wi: NT / 32.
-// Ends without a barrier: the caller's next barrier must come before X or ro
-// is written again.
+// Steps (2)-(4) for player q at a unit of n_it (1 or 2) terminals that share
+// the opponent reach ro (sibling terminals below a node where q acts: a fold
+// and a call, whose opponent reach is the node's), staged in shared memory
+// (16-byte aligned, zero past Ho up to a multiple of 4), whose absolute mass
+// S the caller has reduced.  One scan serves the unit: over all three lists
+// if it holds a showdown, else over the per-card lists.  X: 3 * Ho + 8 ints;
+// wi: NT / 32.  Ends without a barrier: the caller's next barrier must come
+// before X or ro is written again.
 template <int NT>
-__device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, const float* __restrict__ ro, float S,
-                                float* __restrict__ out, int* X, int* wi, FxCards* cd, int semantics, int tid) {
+__device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxItem& it1, int n_it, const TabView& tv, int q,
+                                const float* __restrict__ ro, float S, int* X, int* wi, FxCards* cd, int semantics,
+                                int tid) {
     static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
     const int o = 1 - q;
     const int Ho = ti.H[o], Hpq = ti.Hp[q];
-    const bool fold = ti.type == MTT_NODE_FOLD;
-    const int lo = fold ? Ho : 0;            // folds scan only the per-card lists
+    const bool need_A = it0.type != MTT_NODE_FOLD || (n_it > 1 && it1.type != MTT_NODE_FOLD);
+    const int lo = need_A ? 0 : Ho;          // folds alone scan only the per-card lists
     const int N = 3 * Ho - lo;
     const uint16_t* idx = tv.sorted[o] + lo; // [rank order (Ho) | per-card lists (2 Ho)], contiguous
     const FxScale fs = fx_scale(S);
@@ -477,18 +502,31 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const TabView& tv, int q, co
     __syncthreads();
     FxEval ev;
     ev.ent = tv.ent[q]; ev.cd = cd; ev.X = X; ev.ro = ro; ev.fs = fs;
-    ev.Tt = (unsigned)(fold ? total >> 1 : X[Ho]);   // total is even: exact halving
-    const float cq = ti.c[q], pot = ti.pot;
-    ev.ga = __fmul_rn(__fmul_rn(0.5f, pot), fs.inv);
-    ev.gc = __fmul_rn(cq, fs.inv);
-    ev.gp = __fmul_rn((q == ((ti.wmask == 1) ? 0 : 1)) ? pot - cq : -cq, fs.inv);
-    ev.Hq = ti.H[q]; ev.q = q; ev.semantics = semantics; ev.fold = fold;
+    ev.Tt = (unsigned)(need_A ? X[Ho] : total >> 1);   // a fold scan's total is even: exact halving
+    ev.Hq = ti.H[q]; ev.q = q; ev.semantics = semantics; ev.need_A = need_A;
+    float ga[2], gc[2], gp[2];
+    bool fd[2];
+    float* out[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const FxItem& it = (i == 1 && n_it > 1) ? it1 : it0;
+        const float cq = q ? it.c1 : it.c0;
+        ga[i] = __fmul_rn(__fmul_rn(0.5f, it.pot), fs.inv);
+        gc[i] = __fmul_rn(cq, fs.inv);
+        gp[i] = __fmul_rn((q == ((it.wmask == 1) ? 0 : 1)) ? it.pot - cq : -cq, fs.inv);
+        fd[i] = it.type == MTT_NODE_FOLD;
+        out[i] = it.out;
+    }
     // two hands per step: their dependent shared-memory chains overlap
     for (int h = tid; h < Hpq; h += 2 * NT) {
-        const float v0 = ev(h);
-        const float v1 = ev(h + NT);
-        out[h] = v0;
-        if (h + NT < Hpq) out[h + NT] = v1;
+        const FxHand x0 = ev.hand(h), x1 = ev.hand(h + NT);
+        const bool in1 = h + NT < Hpq;
+        out[0][h] = ev.value(x0, fd[0], ga[0], gc[0], gp[0]);
+        if (in1) out[0][h + NT] = ev.value(x1, fd[0], ga[0], gc[0], gp[0]);
+        if (n_it > 1) {
+            out[1][h] = ev.value(x0, fd[1], ga[1], gc[1], gp[1]);
+            if (in1) out[1][h + NT] = ev.value(x1, fd[1], ga[1], gc[1], gp[1]);
+        }
     }
 }
 
@@ -804,13 +842,28 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
             return;
         }
     }
-    for (int t = 0; t < g.count; ++t) {
-        const int s = t & 1;
-        // stage s ^ 1 was last read by terminal t - 1, which ended on a barrier
-        if (tid == 0 && t + 1 < g.count) issue_reach(t + 1, s ^ 1);
-        const TermItem& it = items[g.first + t];
-        ti.pot = it.pot; ti.c[0] = it.c0; ti.c[1] = it.c1;
-        ti.type = it.type_wmask & 0xFF; ti.wmask = (it.type_wmask >> 8) & 0xFF;
+    // Units: a terminal, or two adjacent ones (siblings) whose opponent reach
+    // for the updated player is the same vector (one direction only).
+    auto unit_len = [&](int t) -> int {
+        if (both || t + 1 >= g.count) return 1;
+        const int o = 1 - q1;
+        return items[g.first + t + 1].ro[o] == items[g.first + t].ro[o] ? 2 : 1;
+    };
+    int t = 0, len = unit_len(0);
+    for (int u = 0; t < g.count; ++u) {
+        const int s = u & 1;
+        const int tn = t + len;                  // the next unit's first terminal
+        // stage s ^ 1 was last read by the previous unit, which ended on a barrier
+        if (tid == 0 && tn < g.count) issue_reach(tn, s ^ 1);
+        FxItem f0, f1;
+        auto load_item = [&](FxItem& f, const TermItem& it) {
+            f.pot = it.pot; f.c0 = it.c0; f.c1 = it.c1;
+            f.type = it.type_wmask & 0xFF; f.wmask = (it.type_wmask >> 8) & 0xFF;
+        };
+        const TermItem& ia = items[g.first + t];
+        const TermItem& ib = items[g.first + t + (len > 1 ? 1 : 0)];
+        load_item(f0, ia);
+        load_item(f1, ib);
         const float* st = s ? Rst1 : Rst0;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -818,12 +871,15 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
             float S = 0.f;
 #pragma unroll
             for (int k = 0; k < TG / 32; ++k) S += wf[s][q][k];
+            f0.out = a.arena + ia.out[q];
+            f1.out = a.arena + ib.out[q];
             if (both && q == 1) __syncthreads();   // player 0's values have been read out of X
-            cta_terminal_fx<TG>(ti, tv, q, opp(st, q), S, a.arena + it.out[q], X, wi, &cards, a.semantics, tid);
+            cta_terminal_fx<TG>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, a.semantics, tid);
         }
-        // terminal t + 1's reach and masses; the barrier also ends terminal t
+        // the next unit's reach and masses; the barrier also ends this unit
+        const int lenn = tn < g.count ? unit_len(tn) : 0;
         bool ok = true;
-        if (t + 1 < g.count) {
+        if (tn < g.count) {
             ok = mbar_wait_bounded(&bar[2 - s], (parity >> (s ^ 1)) & 1u);
             parity ^= 1u << (s ^ 1);
             if (ok) mass_parts(s ? Rst0 : Rst1, s ^ 1);
@@ -832,6 +888,8 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
             if (tid == 0) atomicOr(a.err, 1);
             return;
         }
+        t = tn;
+        len = lenn;
     }
 }
 
