@@ -52,6 +52,10 @@ const char* mtt_version(void);
 #define MTT_NODE_FOLD     1
 #define MTT_NODE_SHOWDOWN 2
 #define MTT_NODE_CHANCE   3
+/* Depth-limit leaf (no reference counterpart): the turn betting round closed
+ * with chips behind; the river that follows is valued by a leaf network
+ * (mtt_batch_set_leafnet).  reserved = the chips each player has behind. */
+#define MTT_NODE_LEAF     4
 
 /* Flat heads-up tree node, 32 bytes.  The field order, widths and meaning
  * follow the reference's FlatNode (src/postflop/honest_multistreet_solver.cu:14-21):
@@ -95,6 +99,8 @@ typedef struct mtt_tree_spec {
     int32_t raise_cap;
     int32_t allin;                      /* 1: all-in is always offered */
     int32_t street;                     /* 5 or 4 */
+    int32_t river_leaves;               /* street 4: rounds that close with chips behind end in
+                                           MTT_NODE_LEAF instead of a river chance node */
 } mtt_tree_spec;
 
 /* Build the tree in breadth-first order (children contiguous, parents first).
@@ -218,6 +224,7 @@ typedef struct mtt_subgame {
 } mtt_subgame;
 
 typedef struct mtt_batch mtt_batch;
+typedef struct mtt_leafnet mtt_leafnet;   /* the leaf network (declared with its functions below) */
 
 /* Pack n subgames (host pointers) into device memory on the current device.
  * Synchronous.  Per subgame the layout is reach/CFV vectors per node, R and S
@@ -288,6 +295,19 @@ int mtt_batch_check(mtt_batch* b, void* stream);
 /* Kernels launched for this batch since it was created; a graph replay counts
  * every kernel node it runs. No reference counterpart (instrumentation). */
 int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
+/* Depth-limit leaves (MTT_NODE_LEAF, turn subgames): every pass of every
+ * iteration values them by the leaf network `net` (whose batch capacity must
+ * hold 48 rows per leaf of the batch) on both players' current reach, per
+ * river card, and averages the river cards as a river chance node does
+ * (divisor 44, or 46 in the reference semantics).  flags:
+ * MTT_LEAF_VALUES_RESIDUAL adds the check-down values of the same ranges to
+ * the network's output (a network trained on the residual); net == NULL
+ * values the leaves by check-down alone.  Required before solving a batch
+ * with leaves; such a batch has no best response (exploitability must be 0),
+ * no kernel profile and no ev_grad.  The network stays owned by the caller
+ * and must outlive the solves.  No reference counterpart. */
+#define MTT_LEAF_VALUES_RESIDUAL 1
+int mtt_batch_set_leafnet(mtt_batch* b, mtt_leafnet* net, int32_t flags);
 /* Runs `iters` CFR iterations (no best response, no graph) with a CUDA event
  * around each kernel class of every pass and returns, per iteration,
  * h_ms[3] = device time and h_bytes[3] = compulsory bytes (every element a
@@ -323,12 +343,13 @@ int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, vo
 #define MTT_LEAF_IN     2706
 #define MTT_LEAF_HIDDEN 1024
 #define MTT_LEAF_OUT    2652
-typedef struct mtt_leafnet mtt_leafnet;
 #define MTT_LEAF_ZERO_OUTPUT 1   /* flags: start the output layer at zero (a residual on a base estimate) */
 /* batch_cap: largest batch (multiple of 8).  He-initialised from seed. */
 int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, int32_t flags, mtt_leafnet** out);
 /* d_x [M][2706] float features -> d_y [M][2652] float predictions. */
 int mtt_leafnet_forward(mtt_leafnet* n, const float* d_x, int32_t M, float* d_y, void* stream);
+/* *cap = the largest batch (rows) the network was created for. */
+int mtt_leafnet_capacity(mtt_leafnet* n, int32_t* cap);
 /* Gradients of the masked mean squared error sum(w (y - t)^2) / (M * 2652)
  * for targets d_t [M][2652] and weights d_w (NULL = all ones); *h_loss gets
  * the loss (synchronises when h_loss is given).  M a multiple of 8. */

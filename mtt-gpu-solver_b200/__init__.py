@@ -11,7 +11,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (ALGO_CFRPLUS, ALGO_DCFR, NODE_CHANCE, NODE_DECISION, NODE_DTYPE, NODE_FOLD,
+from ._lib import (ALGO_CFRPLUS, ALGO_DCFR, NODE_CHANCE, NODE_DECISION, NODE_DTYPE, NODE_FOLD, NODE_LEAF,
                    NODE_SHOWDOWN, SEM_CORRECT, SEM_REFERENCE, MttError, SolveParams, Subgame, TreeSpec,
                    check, lib)
 
@@ -45,7 +45,7 @@ def live_combos(board):
 
 
 # ------------------------------------------------------------------ trees
-def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5):
+def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, river_leaves=False):
     sp = TreeSpec()
     sp.pot = float(pot)
     sp.stack = float(stack)
@@ -59,12 +59,16 @@ def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, 
     sp.raise_cap = int(raise_cap)
     sp.allin = 1 if allin else 0
     sp.street = int(street)
+    sp.river_leaves = 1 if river_leaves else 0
     return sp
 
 
-def build_tree(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, board=None):
-    """Betting tree as a NODE_DTYPE array plus (rows0, rows1) and max depth."""
-    sp = make_spec(pot, stack, bet_sizes, raise_sizes, raise_cap, allin, street)
+def build_tree(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, board=None,
+               river_leaves=False):
+    """Betting tree as a NODE_DTYPE array plus (rows0, rows1) and max depth.
+    river_leaves (turn trees): rounds that close with chips behind end in a
+    NODE_LEAF valued by a leaf network instead of a river chance node."""
+    sp = make_spec(pot, stack, bet_sizes, raise_sizes, raise_cap, allin, street, river_leaves)
     L = lib()
     n = ctypes.c_int32()
     rows = (ctypes.c_int32 * 2)()
@@ -328,6 +332,17 @@ class RiverBatch:
         n = ctypes.c_int64()
         check("mtt_batch_launch_count", lib().mtt_batch_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+    def set_leafnet(self, net=None, residual=True):
+        """Values the batch's depth-limit leaves (NODE_LEAF) by the leaf
+        network `net` (a leafnet.LeafNet whose batch capacity holds 48 rows
+        per leaf), as a residual over the check-down values when `residual`;
+        net=None values them by check-down alone.  The network must outlive
+        the solves."""
+        h = net._h if net is not None else None
+        flags = 1 if (net is not None and residual) else 0
+        check("mtt_batch_set_leafnet", lib().mtt_batch_set_leafnet(self._h, h, flags))
+        self._leafnet = net
 
     def kernel_profile(self, params, iters=10, stream=None):
         """Per-iteration device time (ms) and compulsory bytes of the forward

@@ -15,7 +15,7 @@ MTT_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "timeout", 5: "io",
           6: "unsupported"}
 
-NODE_DECISION, NODE_FOLD, NODE_SHOWDOWN, NODE_CHANCE = 0, 1, 2, 3
+NODE_DECISION, NODE_FOLD, NODE_SHOWDOWN, NODE_CHANCE, NODE_LEAF = 0, 1, 2, 3, 4
 ALGO_CFRPLUS, ALGO_DCFR = 0, 1
 SEM_CORRECT, SEM_REFERENCE = 0, 1
 
@@ -32,7 +32,8 @@ class TreeSpec(ctypes.Structure):
     _fields_ = [("pot", ctypes.c_float), ("stack", ctypes.c_float),
                 ("n_bet_sizes", ctypes.c_int32), ("bet_sizes", ctypes.c_float * 8),
                 ("n_raise_sizes", ctypes.c_int32), ("raise_sizes", ctypes.c_float * 8),
-                ("raise_cap", ctypes.c_int32), ("allin", ctypes.c_int32), ("street", ctypes.c_int32)]
+                ("raise_cap", ctypes.c_int32), ("allin", ctypes.c_int32), ("street", ctypes.c_int32),
+                ("river_leaves", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):
@@ -114,6 +115,8 @@ def lib():
         "mtt_batch_root_values": ([vp, i32, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_launch_count": ([vp, vp], ctypes.c_int),
         "mtt_batch_kernel_profile": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_batch_set_leafnet": ([vp, vp, i32], ctypes.c_int),
+        "mtt_leafnet_capacity": ([vp, vp], ctypes.c_int),
         "mtt_batch_layout": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_ev_grad": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_check": ([vp, vp], ctypes.c_int),

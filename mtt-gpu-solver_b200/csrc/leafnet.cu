@@ -324,6 +324,12 @@ extern "C" int mtt_leafnet_forward(mtt_leafnet* n, const float* d_x, int32_t M, 
     return MTT_OK;
 }
 
+extern "C" int mtt_leafnet_capacity(mtt_leafnet* n, int32_t* cap) {
+    if (!n || !cap) return MTT_ERR_INVALID;
+    *cap = n->cap;
+    return MTT_OK;
+}
+
 extern "C" int mtt_leafnet_gradients(mtt_leafnet* n, const float* d_x, const float* d_y, const float* d_w, int32_t M,
                                      double* h_loss, void* stream) {
     if (!n || !d_x || !d_y || (M % 8)) return MTT_ERR_INVALID;

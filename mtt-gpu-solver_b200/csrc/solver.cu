@@ -1000,6 +1000,196 @@ __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __res
     }
 }
 
+// ------------------------------------------------------------- depth-limit leaves
+// A leaf (MTT_NODE_LEAF) ends a turn betting round that closed with chips
+// behind; in the full game the river is dealt and played out.  Its values
+// are built per river card c (48 rows per leaf) from both players' reach at
+// the leaf with the combos holding c removed:
+//  * the check-down value: the showdown of the pot at that reach, from the
+//    turn subgame's table variant of c by the fixed-point terminal routine
+//    (card removal, split ties), in chips;
+//  * optionally the leaf network's correction: both reaches normalised to
+//    ranges over the 1,326 combos and fed as in its training (each range
+//    scaled by the 1,081 combos live on a river board, the 5-card board
+//    one-hot, pot 1 and chips behind / pot); its output, in units of the
+//    pot with both ranges summing to 1, times pot x the opponent's mass.
+// Player q's value of hand h at the leaf is the sum over c not in h of those
+// values, divided by the river chance divisor of the solver's semantics (44
+// correct, 46 reference), as a river chance node of the full tree averages
+// its children.  The check-down part always uses the correct semantics, the
+// basis the network was trained on.
+struct alignas(16) LeafItem {
+    long long reach[2];   // arena float offsets of each player's reach at the leaf
+    long long cfv[2];     // arena float offsets (value region) of each player's values at the leaf
+    long long hc[2];      // hand-card offsets of each player
+    long long tab;        // byte offset of the subgame's table variants (variant c = river card c)
+    float pot, spr;       // chips in the pot; chips behind / pot
+    int H[2], Hp[2];
+    int row0;             // first row of the leaf
+    int vsize;            // bytes per table variant
+    uint8_t board[4];
+    int sub;
+};
+
+constexpr int LEAF_RIVERS = 48;        // river cards after a 4-card board
+constexpr int LEAF_IN = 2706, LEAF_OUT = 2652, LEAF_COMBOS = 1326;
+
+__device__ __forceinline__ int combo_index(int a, int b) {   // a < b, lexicographic pairs
+    return a * 51 - a * (a - 1) / 2 + (b - a - 1);
+}
+
+// The j-th card (ascending) not on the 4-card board.
+__device__ __forceinline__ int leaf_river_card(const uint8_t* bd, int j) {
+    int k = -1;
+    for (int x = 0; x < 52; ++x) {
+        if (x == bd[0] || x == bd[1] || x == bd[2] || x == bd[3]) continue;
+        if (++k == j) return x;
+    }
+    return -1;
+}
+
+// Shared memory of k_leaf_showdown for one leaf and updated player q.
+__host__ __device__ inline int leaf_sd_smem(int Ho, int Hq, int Hpo) {
+    return tab_idx_bytes(Ho) + tab_ent_bytes(Hq) + 4 * Hpo + 4 * (3 * Ho + 8) + 16;
+}
+
+// One network row (leaf, river card) per CTA: features X [rows][2706] and
+// reach masses M [rows][2].
+__global__ void __launch_bounds__(256) k_leaf_rows(SolveDev a, const LeafItem* __restrict__ leaves, float* __restrict__ X,
+                                                   float* __restrict__ M) {
+    __shared__ float wsum[8];
+    const int row = blockIdx.x, tid = threadIdx.x;
+    const LeafItem L = leaves[row / LEAF_RIVERS];
+    const int c = leaf_river_card(L.board, row % LEAF_RIVERS);
+    float* x = X + (size_t)row * LEAF_IN;
+    for (int i = tid; i < LEAF_IN; i += 256) x[i] = 0.0f;
+    __syncthreads();
+    for (int p = 0; p < 2; ++p) {
+        const float* rp = a.arena + L.reach[p];
+        const uint16_t* hc = a.hcards + L.hc[p];
+        float part = 0.0f;
+        for (int h = tid; h < L.H[p]; h += 256) {
+            const int cc = hc[h];
+            if ((cc & 0xFF) != c && (cc >> 8) != c) part += rp[h];
+        }
+        part = warp_sum(part);
+        if ((tid & 31) == 0) wsum[tid >> 5] = part;
+        __syncthreads();
+        float tot = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tot += wsum[k];
+        __syncthreads();
+        const float inv = tot > 0.0f ? 1.0f / tot : 0.0f;
+        for (int h = tid; h < L.H[p]; h += 256) {
+            const int cc = hc[h], c1 = cc & 0xFF, c2 = cc >> 8;
+            if (c1 == c || c2 == c) continue;
+            x[p * LEAF_COMBOS + combo_index(c1, c2)] = rp[h] * inv * 1081.0f;
+        }
+        if (tid == 0) M[2 * (size_t)row + p] = tot;
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 4; ++k) x[2 * LEAF_COMBOS + L.board[k]] = 1.0f;
+        x[2 * LEAF_COMBOS + c] = 1.0f;
+        x[2 * LEAF_COMBOS + 52] = 1.0f;       // pot / 100 with the pot scaled to 100
+        x[2 * LEAF_COMBOS + 53] = L.spr;      // stack / 100 at that scale
+    }
+}
+
+// Check-down values (chips) of one (leaf, river card) row per CTA for the
+// updated players `upd`: SD[row][q][0..Hp_q), row stride 2 * sd_stride.
+__global__ void __launch_bounds__(TG) k_leaf_showdown(SolveDev a, const LeafItem* __restrict__ leaves,
+                                                      float* __restrict__ SD, int sd_stride, int upd) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ float wf[TG / 32];
+    __shared__ int wi[TG / 32];
+    __shared__ FxCards cards;
+    const int row = blockIdx.x, tid = threadIdx.x;
+    const LeafItem L = leaves[row / LEAF_RIVERS];
+    const int c = leaf_river_card(L.board, row % LEAF_RIVERS);
+    const uint8_t* var = a.tabs + L.tab + (size_t)c * L.vsize;
+    for (int q = 0; q < 2; ++q) {
+        if (!((upd >> q) & 1)) continue;
+        const int o = 1 - q, Ho = L.H[o];
+        const int ib = tab_idx_bytes(Ho), eb = tab_ent_bytes(L.H[q]);
+        uint8_t* T = smem;
+        const uint4* si = reinterpret_cast<const uint4*>(var + tab_idx_off(o, L.H[0]));
+        const uint4* se = reinterpret_cast<const uint4*>(var + tab_ent_off(q, L.H[0], L.H[1]));
+        for (int i = tid; i < ib / 16; i += TG) reinterpret_cast<uint4*>(T)[i] = si[i];
+        for (int i = tid; i < eb / 16; i += TG) reinterpret_cast<uint4*>(T + ib)[i] = se[i];
+        // opponent reach, without the combos the river card removes (zero past Ho)
+        float* ro = reinterpret_cast<float*>(T + ib + eb);
+        const float* rs = a.arena + L.reach[o];
+        const uint16_t* hc = a.hcards + L.hc[o];
+        for (int j = tid; j < L.Hp[o]; j += TG) {
+            float r = 0.0f;
+            if (j < Ho) {
+                const int cc = hc[j];
+                if ((cc & 0xFF) != c && (cc >> 8) != c) r = rs[j];
+            }
+            ro[j] = r;
+        }
+        int* X = reinterpret_cast<int*>(T + ib + eb + 4 * L.Hp[o]);
+        __syncthreads();
+        const float part = fx_abs_part<TG>(ro, Ho, tid);
+        if ((tid & 31) == 0) wf[tid >> 5] = part;
+        __syncthreads();
+        float S = 0.0f;
+#pragma unroll
+        for (int k = 0; k < TG / 32; ++k) S += wf[k];
+        TabView tv;
+        const uint16_t *so, *co, *sg;
+        tab_idx_view(T, Ho, &so, &co, &sg);
+        tv.sorted[0] = tv.sorted[1] = so;
+        tv.cl[0] = tv.cl[1] = co;
+        tv.seg[0] = tv.seg[1] = sg;
+        tv.ent[0] = tv.ent[1] = reinterpret_cast<const Entry*>(T + ib);
+        TermInfo ti;
+        ti.H[0] = L.H[0]; ti.H[1] = L.H[1]; ti.Hp[0] = L.Hp[0]; ti.Hp[1] = L.Hp[1];
+        FxItem it;
+        it.out = SD + ((size_t)row * 2 + q) * sd_stride;
+        it.pot = L.pot; it.c0 = 0.5f * L.pot; it.c1 = 0.5f * L.pot;
+        it.type = MTT_NODE_SHOWDOWN; it.wmask = 3;
+        cta_terminal_fx<TG>(ti, it, it, 1, tv, q, ro, S, X, wi, &cards, MTT_SEM_CORRECT, tid);
+        __syncthreads();   // the next player restages shared memory
+    }
+}
+
+// Leaf values of the updated players `upd` from the check-down values SD
+// and/or the network output Y with the masses M (either source may be null).
+__global__ void __launch_bounds__(256) k_leaf_values(SolveDev a, const LeafItem* __restrict__ leaves,
+                                                     const float* __restrict__ SD, int sd_stride,
+                                                     const float* __restrict__ Y, const float* __restrict__ M, int upd,
+                                                     float div) {
+    __shared__ int rc[LEAF_RIVERS];
+    const int tid = threadIdx.x;
+    const LeafItem L = leaves[blockIdx.x];
+    if (tid < LEAF_RIVERS) rc[tid] = leaf_river_card(L.board, tid);
+    __syncthreads();
+    for (int q = 0; q < 2; ++q) {
+        if (!((upd >> q) & 1)) continue;
+        const int o = 1 - q;
+        float* out = a.arena + L.cfv[q];
+        const uint16_t* hc = a.hcards + L.hc[q];
+        for (int h = tid; h < L.Hp[q]; h += 256) {
+            float v = 0.0f;
+            if (h < L.H[q]) {
+                const int cc = hc[h], c1 = cc & 0xFF, c2 = cc >> 8;
+                const int id = q * LEAF_COMBOS + combo_index(c1, c2);
+                float acc = 0.0f;
+                for (int j = 0; j < LEAF_RIVERS; ++j) {
+                    if (rc[j] == c1 || rc[j] == c2) continue;
+                    const size_t row = (size_t)L.row0 + j;
+                    float y = SD ? SD[(row * 2 + q) * sd_stride + h] : 0.0f;
+                    if (Y) y = fmaf(__fmul_rn(L.pot, M[2 * row + o]), Y[row * LEAF_OUT + id], y);
+                    acc += y;
+                }
+                v = __fdiv_rn(acc, div);
+            }
+            out[h] = v;
+        }
+    }
+}
+
 // ------------------------------------------------------------- differentiable EV
 // Fixed strategies sigma = softmax(logits) per node and hand; the logits sit
 // in the regret layout (a.R) and dEV0/dlogits is written in the same layout
@@ -1413,6 +1603,16 @@ struct mtt_batch {
     mtt_solve_params gparams{};
     int gthreads = 0;
     mutable long long launches = 0;    // kernels run for this batch (graph replays count every node)
+    // depth-limit leaves (turn subgames built with river_leaves)
+    std::vector<mtt::LeafItem> h_leaves;
+    mtt::LeafItem* d_leaves = nullptr;
+    int n_leaves = 0;
+    bool leaf_ready = false;           // mtt_batch_set_leafnet was called
+    mtt_leafnet* net = nullptr;
+    bool leaf_residual = false;
+    float *d_lx = nullptr, *d_ly = nullptr, *d_lm = nullptr, *d_lsd = nullptr;
+    int leaf_sd_stride = 0;            // floats per (row, player) of d_lsd
+    int leaf_smem = 0;                 // dynamic shared memory of k_leaf_showdown
 };
 
 namespace mtt {
@@ -1438,6 +1638,7 @@ static void free_batch(mtt_batch* b) {
     cudaFree(b->d_ranges); cudaFree(b->d_arena); cudaFree(b->d_R); cudaFree(b->d_S);
     cudaFree(b->d_darena); cudaFree(b->d_results); cudaFree(b->d_iter); cudaFree(b->d_iter_tab);
     cudaFree(b->d_err);
+    cudaFree(b->d_leaves); cudaFree(b->d_lx); cudaFree(b->d_ly); cudaFree(b->d_lm); cudaFree(b->d_lsd);
     free_set(b->full);
     free_set(b->act);
     delete b;
@@ -1614,17 +1815,46 @@ static int launch_term(const mtt_batch* b, const ListSet& L, const SolveDev& a, 
     return MTT_OK;
 }
 
-// One CFR iteration: per pass forward levels, terminals, backward levels.
+// Depth-limit leaves of the updated players `upd`: the network's rows and
+// forward pass (with a network), the check-down values (unless the network
+// alone values them), then the leaf values.
+static int launch_leaves(const mtt_batch* b, const SolveDev& a, int upd, cudaStream_t st) {
+    if (!b->n_leaves) return MTT_OK;
+    const int rows = LEAF_RIVERS * b->n_leaves;
+    if (b->net) {
+        k_leaf_rows<<<rows, 256, 0, st>>>(a, b->d_leaves, b->d_lx, b->d_lm);
+        MTT_CHECK_LAUNCH();
+        ++b->launches;
+        MTT_TRY(mtt_leafnet_forward(b->net, b->d_lx, rows, b->d_ly, (void*)st));
+        b->launches += 5;   // feature packing and four GEMMs
+    }
+    const bool cd = b->leaf_residual || !b->net;
+    if (cd) {
+        k_leaf_showdown<<<rows, TG, b->leaf_smem, st>>>(a, b->d_leaves, b->d_lsd, b->leaf_sd_stride, upd);
+        MTT_CHECK_LAUNCH();
+        ++b->launches;
+    }
+    const float div = (float)(LEAF_RIVERS - 4 + (a.semantics ? 2 : 0));
+    k_leaf_values<<<b->n_leaves, 256, 0, st>>>(a, b->d_leaves, cd ? b->d_lsd : nullptr, b->leaf_sd_stride,
+                                               b->net ? b->d_ly : nullptr, b->d_lm, upd, div);
+    MTT_CHECK_LAUNCH();
+    ++b->launches;
+    return MTT_OK;
+}
+
+// One CFR iteration: per pass forward levels, leaves, terminals, backward levels.
 static int launch_iteration(const mtt_batch* b, const ListSet& L, const SolveDev& a, const mtt_solve_params& p,
                             int threads, cudaStream_t st) {
     if (p.alternate) {
         for (int u = 0; u < 2; ++u) {
             MTT_TRY(launch_levels_fwd(b, a, L.f_alt[u], threads, st));
+            MTT_TRY(launch_leaves(b, a, 1 << u, st));
             MTT_TRY(launch_term(b, L, a, 1 << u, st));
             MTT_TRY(launch_levels_bwd(b, a, L.b_alt[u], threads, st));
         }
     } else {
         MTT_TRY(launch_levels_fwd(b, a, L.f_sim, threads, st));
+        MTT_TRY(launch_leaves(b, a, 3, st));
         MTT_TRY(launch_term(b, L, a, 3, st));
         MTT_TRY(launch_levels_bwd(b, a, L.b_sim, threads, st));
     }
@@ -1744,6 +1974,8 @@ static int run_iterations(mtt_batch* b, const ListSet& L, const SolveDev& a, con
 }
 
 static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, bool graph) {
+    if (b->n_leaves && !b->leaf_ready) return MTT_ERR_INVALID;        // leaf values undefined
+    if (b->n_leaves && p.exploitability) return MTT_ERR_UNSUPPORTED;  // no best response through leaves
     const int threads = p.threads ? p.threads : (b->tuned_threads ? b->tuned_threads : 256);
     const bool gate = p.exploitability && p.target_expl > 0.0f && p.max_iters > p.iters;
     const int chunk = p.chunk_iters > 0 ? p.chunk_iters : std::max(p.iters / 2, 1);
@@ -1816,6 +2048,7 @@ extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* pr
                                         double* h_bytes, void* stream) {
     using namespace mtt;
     if (!b || !h_ms || !h_bytes || iters <= 0) return MTT_ERR_INVALID;
+    if (b->n_leaves) return MTT_ERR_UNSUPPORTED;
     MTT_TRY(check_params(prm));
     const mtt_solve_params& p = *prm;
     cudaStream_t st = as_stream(stream);
@@ -2027,6 +2260,23 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                 }
                 addT(HL.bf[dp], gn, i, Hmax);
                 addT(HL.bb[dp], gn, i, Hmax);
+            } else if (nd.type == MTT_NODE_LEAF) {
+                LeafItem lf{};
+                for (int p = 0; p < 2; ++p) {
+                    lf.reach[p] = reach0 + src[p] * HS + off[p];
+                    lf.cfv[p] = cfv0 + (long long)k * HS + off[p];
+                    lf.hc[p] = d.hcard_base + off[p];
+                    lf.H[p] = Hh[p];
+                    lf.Hp[p] = Hp[p];
+                }
+                lf.pot = nd.pot;
+                lf.spr = nd.pot > 0.0f ? subs[i].nodes[k].reserved / nd.pot : 0.0f;
+                lf.row0 = LEAF_RIVERS * (int)b->h_leaves.size();
+                lf.tab = d.tab_base;
+                lf.vsize = d.tab_vsize;
+                lf.sub = i;
+                for (int c = 0; c < 4; ++c) lf.board[c] = subs[i].board[c];
+                b->h_leaves.push_back(lf);
             } else {
                 HL.terms.push_back(make_int2(gn, i));
                 TermItem t{};
@@ -2066,6 +2316,12 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
     if (!s) s = dalloc(&b->d_err, 1, total);
     if (!s) s = cuda_status(cudaMemset(b->d_err, 0, sizeof(int)));
     if (!s) s = build_set(b, b->full, nullptr, total);
+    b->n_leaves = (int)b->h_leaves.size();
+    if (!s && b->n_leaves) {
+        s = dalloc(&b->d_leaves, b->h_leaves.size(), total);
+        if (!s) s = cuda_status(cudaMemcpy(b->d_leaves, b->h_leaves.data(), sizeof(LeafItem) * b->h_leaves.size(),
+                                           cudaMemcpyHostToDevice));
+    }
     if (s) { free_batch(b); return s; }
     b->device_bytes = total;
     {
@@ -2202,11 +2458,47 @@ extern "C" int mtt_batch_layout(mtt_batch* b, int64_t* h_rows_off, int64_t* h_ra
     return MTT_OK;
 }
 
+extern "C" int mtt_batch_set_leafnet(mtt_batch* b, mtt_leafnet* net, int32_t flags) {
+    using namespace mtt;
+    if (!b || (flags & ~MTT_LEAF_VALUES_RESIDUAL) || !b->n_leaves) return MTT_ERR_INVALID;
+    const long long rows = (long long)LEAF_RIVERS * b->n_leaves;
+    if (net) {
+        int32_t cap = 0;
+        MTT_TRY(mtt_leafnet_capacity(net, &cap));
+        if (rows > cap) return MTT_ERR_INVALID;
+    }
+    if (!b->d_lx) {
+        int stride = 0, smem = 0;
+        for (const LeafItem& lf : b->h_leaves) {
+            stride = std::max(stride, std::max(lf.Hp[0], lf.Hp[1]));
+            for (int q = 0; q < 2; ++q) smem = std::max(smem, leaf_sd_smem(lf.H[1 - q], lf.H[q], lf.Hp[1 - q]));
+        }
+        if (smem > 227 * 1024) return MTT_ERR_UNSUPPORTED;
+        if (smem > 48 * 1024)
+            MTT_TRY_CUDA(cudaFuncSetAttribute(k_leaf_showdown, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        long long total = 0;
+        int s = dalloc(&b->d_lx, (size_t)rows * LEAF_IN, total);
+        if (!s) s = dalloc(&b->d_ly, (size_t)rows * LEAF_OUT, total);
+        if (!s) s = dalloc(&b->d_lm, (size_t)rows * 2, total);
+        if (!s) s = dalloc(&b->d_lsd, (size_t)rows * 2 * stride, total);
+        if (s) return s;
+        b->leaf_sd_stride = stride;
+        b->leaf_smem = smem;
+        b->device_bytes += total;
+    }
+    b->net = net;
+    b->leaf_residual = (flags & MTT_LEAF_VALUES_RESIDUAL) != 0;
+    b->leaf_ready = true;
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }   // captured the old leaf launches
+    return MTT_OK;
+}
+
 extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
                                  float* d_grad_ranges, float* d_grad_logits, void* stream) {
     auto al16 = [](const void* p) { return p && ((uintptr_t)p & 15u) == 0; };
     if (!b || !al16(d_logits) || !al16(d_ranges) || !d_ev || !al16(d_grad_ranges) || !al16(d_grad_logits))
         return MTT_ERR_INVALID;
+    if (b->n_leaves) return MTT_ERR_UNSUPPORTED;
     cudaStream_t st = as_stream(stream);
     mtt_solve_params p{};
     p.algo = MTT_ALGO_CFRPLUS;
@@ -2259,6 +2551,7 @@ extern "C" int mtt_batch_launch_count(mtt_batch* b, int64_t* launches) {
 
 extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads) {
     if (!b) return MTT_ERR_INVALID;
+    if (b->n_leaves && !b->leaf_ready) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
     cudaStream_t st = as_stream(stream);
     mtt_solve_params p = *prm;

@@ -145,7 +145,7 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
         d.c0 = m.committed[0];
         d.c1 = m.committed[1];
         if (m.type == MTT_NODE_DECISION && m.num_actions > MAXA) { sp.status = MTT_ERR_UNSUPPORTED; return; }
-        if (m.type == MTT_NODE_CHANCE && g.nboard != 4) { sp.status = MTT_ERR_INVALID; return; }
+        if ((m.type == MTT_NODE_CHANCE || m.type == MTT_NODE_LEAF) && g.nboard != 4) { sp.status = MTT_ERR_INVALID; return; }
     }
     sp.depth.assign(nn, 0);
     for (int i = 0; i < nn; ++i) {
@@ -175,6 +175,8 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
         sp.nodes[i].dealt = (int16_t)dealt[i];
         // a turn subgame cannot reach a showdown before the river is dealt
         if (g.nboard == 4 && g.nodes[i].type == MTT_NODE_SHOWDOWN && dealt[i] < 0) { sp.status = MTT_ERR_INVALID; return; }
+        // a depth-limit leaf stands for the river deal, so none sits below one
+        if (g.nodes[i].type == MTT_NODE_LEAF && dealt[i] >= 0) { sp.status = MTT_ERR_INVALID; return; }
     }
     // tables
     const int vsize = tab_variant_bytes(H[0], H[1]);

@@ -43,7 +43,7 @@ int build_tree(const mtt_tree_spec& sp, const uint8_t* /*board*/, std::vector<mt
                int rows[2], int* max_depth) {
     if (!(sp.pot > 0.0f) || sp.stack < 0.0f || sp.n_bet_sizes < 0 || sp.n_bet_sizes > MTT_MAX_SIZES ||
         sp.n_raise_sizes < 0 || sp.n_raise_sizes > MTT_MAX_SIZES || sp.raise_cap < 0 ||
-        (sp.street != 4 && sp.street != 5))
+        (sp.street != 4 && sp.street != 5) || (sp.river_leaves && sp.street != 4))
         return MTT_ERR_INVALID;
     for (int i = 0; i < sp.n_bet_sizes; ++i) if (!(sp.bet_sizes[i] > 0.0f)) return MTT_ERR_INVALID;
     for (int i = 0; i < sp.n_raise_sizes; ++i) if (!(sp.raise_sizes[i] > 0.0f)) return MTT_ERR_INVALID;
@@ -183,6 +183,14 @@ int build_tree(const mtt_tree_spec& sp, const uint8_t* /*board*/, std::vector<mt
                 cn.committed[0] = ns.c[0];
                 cn.committed[1] = ns.c[1];
                 if (cn.depth > maxd) maxd = cn.depth;
+            } else if (!all_in && sp.river_leaves) {
+                mtt_node& cn = out[ch];
+                cn.type = MTT_NODE_LEAF;
+                cn.pot_size = ns.c[0] + ns.c[1];
+                cn.committed[0] = ns.c[0];
+                cn.committed[1] = ns.c[1];
+                cn.reserved = std::min(ns.rem[0], ns.rem[1]);   // chips behind at the river
+                if (cn.depth > maxd) maxd = cn.depth;
             } else {
                 BState rs = ns;
                 rs.street = 5;
@@ -299,7 +307,7 @@ int validate_tree(const mtt_node* nodes, int n, const int rows[2]) {
     std::vector<int> parent(n, -1);
     for (int i = 0; i < n; ++i) {
         const mtt_node& nd = nodes[i];
-        if (nd.type > MTT_NODE_CHANCE) return MTT_ERR_INVALID;
+        if (nd.type > MTT_NODE_LEAF) return MTT_ERR_INVALID;
         if (nd.type == MTT_NODE_DECISION || nd.type == MTT_NODE_CHANCE) {
             if (nd.num_actions < 1) return MTT_ERR_INVALID;
             if (nd.children_offset <= i || nd.children_offset + nd.num_actions > n) return MTT_ERR_INVALID;
