@@ -284,6 +284,31 @@ def other_configs(mtt, wl, stream):
     mtt.ev_dump(f4[:8])
     out["ev_dump_1755"] = {"ms": _event_ms(lambda: mtt.ev_dump(f4), stream),
                            "workload": "all 1,755 canonical flops, reference runout subsample (bit-exact dump)"}
+    # depth-limited turn solve: leaf network trained on leaf samples of 64 full solves
+    dlm = importlib.import_module("mtt-gpu-solver_b200.depthlimit")
+    t0 = time.perf_counter()
+    X, T, W, meta = dlm.leaf_training_set(64, seed=100, iters=300)
+    net = dlm.train_on(X, T, W, meta, epochs=3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    spot = dlm.turn_spot(seed=0)
+    res, ms = {}, {}
+    for name, kw in (("full", {"limited": False}), ("net", {"limited": True, "net": net}),
+                     ("checkdown", {"limited": True, "net": None})):
+        dlm.solve(spot, iters=20, **kw)
+        ms[name] = _event_ms(lambda: res.__setitem__(name, dlm.solve(spot, iters=300, **kw)), stream, reps=1)
+    leaf = [dlm.leaf_errors_in_situ(dlm.turn_spot(seed=s), net, iters=300) for s in (0, 1, 2)]
+    out["depth_limited_turn"] = {
+        "solve_ms": {k: v for k, v in ms.items()},
+        "solve_ms_note": "one depthlimit.solve call: tree and table packing, upload, 300 iterations, read-back",
+        "root_value_error_pot": {k: dlm.errors(spot, res[k], res["full"])["value"] for k in ("net", "checkdown")},
+        "leaf_mae_pot": {k: float(np.mean([e[k] for e in leaf])) for k in ("net", "checkdown")},
+        "train_s": train_s, "train_samples": int(len(X)),
+        "workload": "turn spot pot 100, stack 150, bets 50/100% + all-in, 1 raise, Dirichlet(0.3) ranges (1,128 "
+                    "combos), 300 alternating CFR+ iterations: full turn + river tree vs 5 depth-limit leaves valued "
+                    "by check-down (fixed-point scans) or check-down + leaf network; leaf MAE judged at 3 held-out "
+                    "spots' leaves against their full solve"}
+    net.close()
     return out
 
 

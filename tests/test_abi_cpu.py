@@ -110,3 +110,24 @@ def test_workload_config2_shapes(wl):
             assert 200 <= len(c) <= 1081 and (np.diff(c.astype(int)) > 0).all()
             assert (g[f"range{p}"] > 0).all()
         assert g["nodes"]["num_actions"].max() <= 8
+
+
+def test_turn_tree_with_river_leaves(mtt):
+    """Turn rounds that close with chips behind end in NODE_LEAF (chips
+    behind in `reserved`); all-in closes still deal the river to showdowns."""
+    board = [14, 26, 41, 31]
+    full, rows_f, _ = mtt.build_tree(100.0, 150.0, [0.5, 1.0], raise_cap=1, street=4, board=board)
+    lim, rows_l, _ = mtt.build_tree(100.0, 150.0, [0.5, 1.0], raise_cap=1, street=4, board=board, river_leaves=True)
+    assert mtt.validate_tree(lim, rows_l) == 0
+    leaves = lim[lim["type"] == mtt.NODE_LEAF]
+    assert len(leaves) == 5
+    assert sorted({round(float(r) / float(p), 6) for r, p in zip(leaves["reserved"], leaves["pot_size"])}) == \
+        [0.166667, 0.5, 1.5]
+    assert np.all(leaves["committed"][:, 0] == leaves["committed"][:, 1])
+    # the leaf tree keeps the turn rows and drops the river ones
+    n_dec_turn = int(np.sum((lim["type"] == mtt.NODE_DECISION)))
+    assert rows_l[0] + rows_l[1] < rows_f[0] + rows_f[1] and n_dec_turn == 12
+    # every leaf of the limited tree is a river chance node of the full tree
+    assert int(np.sum(full["type"] == mtt.NODE_CHANCE)) == len(leaves) + int(np.sum(lim["type"] == mtt.NODE_CHANCE))
+    with pytest.raises(mtt.MttError):
+        mtt.build_tree(100.0, 150.0, [0.5], street=5, river_leaves=True)
