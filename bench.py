@@ -401,18 +401,30 @@ def run_b200(args, rank, world, local):
     batch.close()
 
     # end to end through the public API from host buffers
+    e2e_parts = {"create": 0.0, "solve": 0.0, "results": 0.0, "close": 0.0}
+
     def e2e_step():
-        b = mtt.RiverBatch(subs)
-        b.solve(p)
-        r = b.results()
+        t = [time.perf_counter()]
+        b = mtt.RiverBatch(subs)                  # pack on host threads, allocate, upload
+        t.append(time.perf_counter())
+        b.solve(p, graph=True)
+        t.append(time.perf_counter())
+        r = b.results()                           # synchronises
+        t.append(time.perf_counter())
         b.close()
+        t.append(time.perf_counter())
+        for k, name in enumerate(("create", "solve", "results", "close")):
+            e2e_parts[name] += t[k + 1] - t[k]
         return r
     e2e_step()
     torch.cuda.synchronize()
+    for k in e2e_parts:
+        e2e_parts[k] = 0.0
     t0 = time.perf_counter()
-    for _ in range(max(1, min(args.steps, 2))):
+    n_e2e = max(1, min(args.steps, 2))
+    for _ in range(n_e2e):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
+    e2e_s = (time.perf_counter() - t0) / n_e2e
     e2e_s = max_over_ranks(e2e_s, pg, "cuda")
     h2d = sum(g["nodes"].nbytes + g["combos0"].nbytes + g["combos1"].nbytes + g["range0"].nbytes +
               g["range1"].nbytes for g in subs)
@@ -472,7 +484,9 @@ def run_b200(args, rank, world, local):
                          "kernel": "CFR sweeps + terminals (k_fwd, k_term, k_bwd), no best response",
                          "peak_kind": peak_kind, "kernel_ms": solve_ms, "per_kernel": kernels},
             "clocks": clocks,
-            "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": args.subgames * world / e2e_s, "unit": "solves/s",
+                    "host_s_per_step": {k: v / n_e2e for k, v in e2e_parts.items()},
+                    "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(args.subgames * 6 * 8)},
             "gpu_launches": int(gpu_launches),
             "other_configs": other}
