@@ -88,7 +88,11 @@ typedef struct mtt_node {
  * above the remaining stack becomes all-in.  raise_cap counts raises after
  * the first bet of a street. street = 5: river subgame (5-card board);
  * street = 4: turn subgame whose betting rounds close into a river chance
- * node (48 children) followed by a river subgame with the same sizes. */
+ * node (48 children) followed by a river subgame with the same sizes;
+ * street = 3: flop subgame (the reference's multistreet structure,
+ * honest_multistreet_solver.cu:97-104,205-219): flop betting, a turn chance
+ * node (49 children), turn betting, then the river dealt (48 children) to
+ * showdowns without river betting. */
 typedef struct mtt_tree_spec {
     float   pot;
     float   stack;
@@ -101,6 +105,8 @@ typedef struct mtt_tree_spec {
     int32_t street;                     /* 5 or 4 */
     int32_t river_leaves;               /* street 4: rounds that close with chips behind end in
                                            MTT_NODE_LEAF instead of a river chance node */
+    int32_t river_runout;               /* street 4: the river is dealt straight to showdowns
+                                           (no river betting); always so for street 3 */
 } mtt_tree_spec;
 
 /* Build the tree in breadth-first order (children contiguous, parents first).
@@ -111,9 +117,12 @@ int mtt_tree_build(const mtt_tree_spec* spec, mtt_node* nodes, int32_t capacity,
 
 /* Turn subgame (spec->street == 4, board = 4 cards): every betting round that
  * closes with chips behind goes to a river chance node with one child per
- * card not on the board, followed by a river round; all-in calls go to a
- * chance node whose children are showdowns.  Also accepts street == 5 with a
- * 5-card board.  Host only. */
+ * card not on the board, followed by a river round (showdowns with
+ * river_runout); all-in calls go to a chance node whose children are
+ * showdowns.  Flop subgame (street == 3, board = 3 cards): the same one street
+ * earlier, with a turn chance node (one child per card not on the board)
+ * before the turn round and the river run out; an all-in deals the turn and
+ * then the river.  Also accepts street == 5 with a 5-card board.  Host only. */
 int mtt_tree_build_board(const mtt_tree_spec* spec, const uint8_t* board, int32_t nboard,
                          mtt_node* nodes, int32_t capacity, int32_t* n_nodes, int32_t rows[2],
                          int32_t* max_depth);

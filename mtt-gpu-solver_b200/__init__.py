@@ -45,7 +45,8 @@ def live_combos(board):
 
 
 # ------------------------------------------------------------------ trees
-def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, river_leaves=False):
+def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, river_leaves=False,
+              river_runout=False):
     sp = TreeSpec()
     sp.pot = float(pot)
     sp.stack = float(stack)
@@ -60,20 +61,24 @@ def make_spec(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, 
     sp.allin = 1 if allin else 0
     sp.street = int(street)
     sp.river_leaves = 1 if river_leaves else 0
+    sp.river_runout = 1 if river_runout else 0
     return sp
 
 
 def build_tree(pot, stack, bet_sizes, raise_sizes=None, raise_cap=1, allin=True, street=5, board=None,
-               river_leaves=False):
+               river_leaves=False, river_runout=False):
     """Betting tree as a NODE_DTYPE array plus (rows0, rows1) and max depth.
-    river_leaves (turn trees): rounds that close with chips behind end in a
-    NODE_LEAF valued by a leaf network instead of a river chance node."""
-    sp = make_spec(pot, stack, bet_sizes, raise_sizes, raise_cap, allin, street, river_leaves)
+    street 5: river; 4: turn (board of 4 cards); 3: flop (board of 3 cards,
+    flop and turn betting, river run out).  river_leaves (turn trees): rounds
+    that close with chips behind end in a NODE_LEAF valued by a leaf network
+    instead of a river chance node.  river_runout (turn trees): the river is
+    dealt straight to showdowns."""
+    sp = make_spec(pot, stack, bet_sizes, raise_sizes, raise_cap, allin, street, river_leaves, river_runout)
     L = lib()
     n = ctypes.c_int32()
     rows = (ctypes.c_int32 * 2)()
     depth = ctypes.c_int32()
-    if street == 4 or board is not None:
+    if street in (3, 4) or board is not None:
         bd = np.ascontiguousarray(np.asarray(board if board is not None else [], dtype=np.uint8))
         check("mtt_tree_build_board", L.mtt_tree_build_board(ctypes.byref(sp), bd.ctypes.data, len(bd), None, 0,
                                                               ctypes.byref(n), rows, ctypes.byref(depth)))

@@ -33,7 +33,7 @@ class TreeSpec(ctypes.Structure):
                 ("n_bet_sizes", ctypes.c_int32), ("bet_sizes", ctypes.c_float * 8),
                 ("n_raise_sizes", ctypes.c_int32), ("raise_sizes", ctypes.c_float * 8),
                 ("raise_cap", ctypes.c_int32), ("allin", ctypes.c_int32), ("street", ctypes.c_int32),
-                ("river_leaves", ctypes.c_int32)]
+                ("river_leaves", ctypes.c_int32), ("river_runout", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):

@@ -38,12 +38,6 @@ namespace mtt {
 
 int validate_tree(const mtt_node* nodes, int n, const int rows[2]);   // tree.cpp
 
-// Table variant of a terminal: river subgames have one board; turn subgames
-// one per dealt river card plus index 52 for nodes before the chance layer
-// (folds there need card lists only, no ranks).
-__host__ __device__ __forceinline__ int tab_variant(int river, int dealt) {
-    return river ? 0 : (dealt < 0 ? 52 : dealt);
-}
 
 // ====================================================================== device
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
@@ -412,12 +406,13 @@ struct FxItem {
 };
 
 // The two integer masses of hand h (step 4); live = false for padding and
-// hands blocked by the dealt card.
+// for hands blocked by a dealt card (blocked = true).
 struct FxHand {
     unsigned A, B;
-    bool live;
+    bool live, blocked;
 };
 
+template <int SEM>   // MTT_SEM_CORRECT or MTT_SEM_REFERENCE
 struct FxEval {
     const Entry* ent;
     const FxCards* cd;
@@ -425,14 +420,14 @@ struct FxEval {
     const float* ro;
     FxScale fs;
     unsigned Tt;
-    int Hq, q, semantics;
+    int Hq, q;
     bool need_A;
 
     __device__ __forceinline__ FxHand hand(int h) const {
-        FxHand x{0u, 0u, false};
+        FxHand x{0u, 0u, false, false};
         if (h >= Hq) return x;
         const Entry et = ent[h];
-        if (et.lt == 0xFFFFu) return x;
+        if (et.lt == 0xFFFFu) { x.blocked = true; return x; }
         x.live = true;
         const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
         x.B = Tt - (unsigned)cd->mass[et.c1] - (unsigned)cd->mass[et.c2] + ps;
@@ -447,9 +442,15 @@ struct FxEval {
 
     // ga = pot/2 * 2^-k, gc = c * 2^-k, gp = fold payoff * 2^-k
     __device__ __forceinline__ float value(const FxHand& x, bool fold, float ga, float gc, float gp) const {
-        if (!x.live) return 0.f;
-        if (fold) return gp * (float)(int)(semantics ? Tt : x.B);
-        if (!semantics) return ga * (float)(int)x.A - gc * (float)(int)x.B;
+        if (!x.live) {
+            // the reference's showdown (no card removal) still meets every
+            // opponent with a hand a dealt card blocks: equity 0, so player 0
+            // loses and player 1 (1 - eq) wins against the whole mass (A = 0)
+            if (!(SEM && x.blocked && !fold)) return 0.f;
+            return ga * (float)(int)(q == 0 ? 0u : 2u * Tt) - gc * (float)(int)Tt;
+        }
+        if (fold) return gp * (float)(int)(SEM ? Tt : x.B);
+        if (!SEM) return ga * (float)(int)x.A - gc * (float)(int)x.B;
         // blocked pairs count as P0 losses (honest:182-187): B = Tt, and
         // player 1's pot share is 2 Lr + T = 2 Tt - A
         const unsigned Aq = q == 0 ? x.A : 2u * Tt - x.A;
@@ -465,10 +466,9 @@ struct FxEval {
 // if it holds a showdown, else over the per-card lists.  X: 3 * Ho + 8 ints;
 // wi: NT / 32.  Ends without a barrier: the caller's next barrier must come
 // before X or ro is written again.
-template <int NT>
+template <int NT, int SEM>
 __device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxItem& it1, int n_it, const TabView& tv, int q,
-                                const float* __restrict__ ro, float S, int* X, int* wi, FxCards* cd, int semantics,
-                                int tid) {
+                                const float* __restrict__ ro, float S, int* X, int* wi, FxCards* cd, int tid) {
     static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
     const int o = 1 - q;
     const int Ho = ti.H[o], Hpq = ti.Hp[q];
@@ -500,10 +500,10 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxI
         cd->mass[tid] = X[cb + seg[tid + 1]] - b;
     }
     __syncthreads();
-    FxEval ev;
+    FxEval<SEM> ev;
     ev.ent = tv.ent[q]; ev.cd = cd; ev.X = X; ev.ro = ro; ev.fs = fs;
     ev.Tt = (unsigned)(need_A ? X[Ho] : total >> 1);   // a fold scan's total is even: exact halving
-    ev.Hq = ti.H[q]; ev.q = q; ev.semantics = semantics; ev.need_A = need_A;
+    ev.Hq = ti.H[q]; ev.q = q; ev.need_A = need_A;
     float ga[2], gc[2], gp[2];
     bool fd[2];
     float* out[2];
@@ -874,7 +874,8 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
             f0.out = a.arena + ia.out[q];
             f1.out = a.arena + ib.out[q];
             if (both && q == 1) __syncthreads();   // player 0's values have been read out of X
-            cta_terminal_fx<TG>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, a.semantics, tid);
+            if (a.semantics) cta_terminal_fx<TG, MTT_SEM_REFERENCE>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, tid);
+            else cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, tid);
         }
         // the next unit's reach and masses; the barrier also ends this unit
         const int lenn = tn < g.count ? unit_len(tn) : 0;
@@ -1149,7 +1150,7 @@ __global__ void __launch_bounds__(TG) k_leaf_showdown(SolveDev a, const LeafItem
         it.out = SD + ((size_t)row * 2 + q) * sd_stride;
         it.pot = L.pot; it.c0 = 0.5f * L.pot; it.c1 = 0.5f * L.pot;
         it.type = MTT_NODE_SHOWDOWN; it.wmask = 3;
-        cta_terminal_fx<TG>(ti, it, it, 1, tv, q, ro, S, X, wi, &cards, MTT_SEM_CORRECT, tid);
+        cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, it, it, 1, tv, q, ro, S, X, wi, &cards, tid);
         __syncthreads();   // the next player restages shared memory
     }
 }
@@ -1404,8 +1405,7 @@ __global__ void __launch_bounds__(TT) k_br_term(SolveDev a, const int2* __restri
     double* reach = a.darena + sd.darena_base;
     double* br = reach + reg;
     double* ev = br + reg;
-    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)tab_variant(sd.river, nd.dealt) * sd.tab_vsize,
-                                sd.H0, sd.H1);
+    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)nd.var * sd.tab_vsize, sd.H0, sd.H1);
     double* X = reinterpret_cast<double*>(smem);
     for (int q = 0; q < 2; ++q) {
         const int o = 1 - q;
@@ -1454,7 +1454,7 @@ __global__ void __launch_bounds__(256) k_br_bwd(SolveDev a, const Task* __restri
     } else if (nd.type == MTT_NODE_CHANCE) {
         const DNode* nodes = a.nodes + sd.node_base;
         const uint16_t* hc = a.hcards + sd.hcard_base;
-        const double div = (double)(sd.n_live - 4);
+        const double div = (double)(nd.nlive - 4);
         for (int q = 0; q < 2; ++q) {
             if (4 * g >= HP(q)) continue;
             for (int i = 0; i < 4; ++i) {
@@ -1495,7 +1495,7 @@ __global__ void __launch_bounds__(TT) k_br_final(SolveDev a, const int* __restri
     z.wmask = 1;
     z.pot = 1.0f;
     z.dealt = -1;
-    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)tab_variant(sd.river, -1) * sd.tab_vsize, sd.H0, sd.H1);
+    const TabView tv = tab_view(a.tabs + sd.tab_base + (size_t)sd.var_none * sd.tab_vsize, sd.H0, sd.H1);
     double* X = reinterpret_cast<double*>(smem);
     double* zm = br + (size_t)nn * HS;
     cta_terminal<double, double, double>(term_info(sd, z), tv, 0, reach + OFF(1), zm, nullptr, X, wb,
@@ -2251,7 +2251,7 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     bw.na = nd.na;
                     bw.flags = BI_CHANCE;
                     bw.first = (int)d.node_base + nd.first;
-                    bw.div = (float)(d.n_live - 4);
+                    bw.div = (float)(nd.nlive - 4);
                     bw.sub = i;
                     for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
                         HL.bsim[dp].push_back(bw);
@@ -2286,7 +2286,7 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     t.H[p] = Hh[p];
                     t.Hp[p] = Hp[p];
                 }
-                t.tab = d.tab_base + (long long)tab_variant(d.river, nd.dealt) * d.tab_vsize;
+                t.tab = d.tab_base + (long long)nd.var * d.tab_vsize;
                 t.pot = nd.pot;
                 t.c0 = nd.c0;
                 t.c1 = nd.c1;

@@ -30,8 +30,9 @@ struct alignas(16) DNode {
     int32_t reach_src0, reach_src1;    // node whose reach slot holds player 0 / 1 reach here
     float pot, c0, c1;
     int16_t dealt;                     // card dealt by the nearest chance ancestor, -1 if none
-    int16_t pad0;
-    int32_t pad1, pad2;
+    int16_t dealt0;                    // card dealt by the chance ancestor above that one, -1 if none
+    int32_t var;                       // showdown table variant of the board this node sees
+    int32_t nlive;                     // chance nodes: cards that can be dealt here
 };
 static_assert(sizeof(DNode) == 48, "DNode is 48 bytes");
 
@@ -48,9 +49,10 @@ struct alignas(16) SubDesc {
     int rows0, rows1;
     int tab_vsize;           // bytes per table variant
     int n_live;              // cards not on the board
-    int river;               // 1: single board (variant 0); 0: variant = dealt card
+    int river;               // 1: single board (variant 0); 0: variants per dealt card(s)
     float pot;               // starting pot (exploitability unit)
-    int pad[3];
+    int var_none;            // table variant of the subgame's own board (no card dealt)
+    int pad[2];
 };
 
 // Table variant layout (bytes), H0/H1 from the descriptor; every block starts

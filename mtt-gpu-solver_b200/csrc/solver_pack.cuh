@@ -1,6 +1,7 @@
 // solver_pack.cuh — host-side packing of heads-up subgames into the device layout
 // of solver_impl.cuh (included by solver.cu only).
 #pragma once
+#include <thread>
 // ====================================================================== host
 struct SubPack {
     std::vector<DNode> nodes;
@@ -16,12 +17,19 @@ static int pad4(int h) { return (h + 3) & ~3; }
 
 static void build_variant(const uint8_t* board, int nboard, int dealt, const int H[2],
                           const std::vector<uint16_t> cards[2], const std::vector<uint16_t> combos[2], uint8_t* out) {
+    // hands holding a board card (a card dealt earlier in a flop subgame) or
+    // the dealt card are blocked: score 0, no entry positions
+    uint64_t bmask = 0;
+    for (int k = 0; k < nboard; ++k) bmask |= 1ull << board[k];
     std::vector<uint32_t> sc[2];
     for (int p = 0; p < 2; ++p) {
         sc[p].resize(H[p]);
         for (int h = 0; h < H[p]; ++h) {
             const int c1 = cards[p][h] & 0xFF, c2 = cards[p][h] >> 8;
-            if (dealt >= 0 && (c1 == dealt || c2 == dealt)) { sc[p][h] = 0u; continue; }
+            if ((dealt >= 0 && (c1 == dealt || c2 == dealt)) || ((bmask >> c1) & 1ull) || ((bmask >> c2) & 1ull)) {
+                sc[p][h] = 0u;
+                continue;
+            }
             Planes pl; planes_clear(pl);
             for (int k = 0; k < nboard; ++k) planes_add(pl, board[k]);
             if (dealt >= 0) planes_add(pl, dealt);
@@ -67,7 +75,7 @@ static void build_variant(const uint8_t* board, int nboard, int dealt, const int
             const int c1 = cards[q][h] & 0xFF, c2 = cards[q][h] >> 8;
             e.c1 = (uint8_t)c1;
             e.c2 = (uint8_t)c2;
-            if (dealt >= 0 && (c1 == dealt || c2 == dealt)) {
+            if ((dealt >= 0 && (c1 == dealt || c2 == dealt)) || ((bmask >> c1) & 1ull) || ((bmask >> c2) & 1ull)) {
                 e.lt = e.le = 0xFFFFu;
                 e.same = -1;
                 ent[h] = e;
@@ -102,7 +110,7 @@ static void combo_cards(int id, int& c1, int& c2) {
 static void pack_one(const mtt_subgame& g, SubPack& sp) {
     sp.status = MTT_OK;
     int rows[2] = {g.rows[0], g.rows[1]};
-    if (!g.nodes || g.n_nodes <= 0 || (g.nboard != 5 && g.nboard != 4)) { sp.status = MTT_ERR_INVALID; return; }
+    if (!g.nodes || g.n_nodes <= 0 || g.nboard < 3 || g.nboard > 5) { sp.status = MTT_ERR_INVALID; return; }
     int st = validate_tree(g.nodes, g.n_nodes, rows);
     if (st) { sp.status = st; return; }
     uint64_t bm = 0;
@@ -131,7 +139,8 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
     const int Hp[2] = {pad4(H[0]), pad4(H[1])};
     // nodes
     sp.nodes.assign(nn, DNode{});
-    std::vector<int> rsrc0(nn, 0), rsrc1(nn, 0), dealt(nn, -1);
+    std::vector<int> rsrc0(nn, 0), rsrc1(nn, 0), dealt(nn, -1), dealt0(nn, -1);
+    std::vector<uint64_t> dm(nn, 0ull);      // cards dealt above (and at) each node
     for (int i = 0; i < nn; ++i) {
         const mtt_node& m = g.nodes[i];
         DNode& d = sp.nodes[i];
@@ -145,7 +154,10 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
         d.c0 = m.committed[0];
         d.c1 = m.committed[1];
         if (m.type == MTT_NODE_DECISION && m.num_actions > MAXA) { sp.status = MTT_ERR_UNSUPPORTED; return; }
-        if ((m.type == MTT_NODE_CHANCE || m.type == MTT_NODE_LEAF) && g.nboard != 4) { sp.status = MTT_ERR_INVALID; return; }
+        if ((m.type == MTT_NODE_CHANCE && g.nboard == 5) || (m.type == MTT_NODE_LEAF && g.nboard != 4)) {
+            sp.status = MTT_ERR_INVALID;
+            return;
+        }
     }
     sp.depth.assign(nn, 0);
     for (int i = 0; i < nn; ++i) {
@@ -158,6 +170,8 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
                 rsrc0[c] = m.player == 0 ? c : rsrc0[i];
                 rsrc1[c] = m.player == 1 ? c : rsrc1[i];
                 dealt[c] = dealt[i];
+                dealt0[c] = dealt0[i];
+                dm[c] = dm[i];
             }
         } else if (m.type == MTT_NODE_CHANCE) {
             for (int k = 0; k < m.num_actions; ++k) {
@@ -165,25 +179,68 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
                 rsrc0[c] = c;
                 rsrc1[c] = c;
                 dealt[c] = g.nodes[c].turn_idx;
-                if (dealt[c] < 0 || dealt[c] > 51 || ((bm >> dealt[c]) & 1ull)) { sp.status = MTT_ERR_INVALID; return; }
+                dealt0[c] = dealt[i];
+                if (dealt[c] < 0 || dealt[c] > 51 || (((bm | dm[i]) >> dealt[c]) & 1ull)) {
+                    sp.status = MTT_ERR_INVALID;
+                    return;
+                }
+                dm[c] = dm[i] | (1ull << dealt[c]);
             }
+            // cards already dealt above a chance node leave no second deal on a 5-card board
+            if (g.nboard + __builtin_popcountll(dm[i]) >= 5) { sp.status = MTT_ERR_INVALID; return; }
         }
     }
     for (int i = 0; i < nn; ++i) {
         sp.nodes[i].reach_src0 = rsrc0[i];
         sp.nodes[i].reach_src1 = rsrc1[i];
         sp.nodes[i].dealt = (int16_t)dealt[i];
-        // a turn subgame cannot reach a showdown before the river is dealt
-        if (g.nboard == 4 && g.nodes[i].type == MTT_NODE_SHOWDOWN && dealt[i] < 0) { sp.status = MTT_ERR_INVALID; return; }
+        sp.nodes[i].dealt0 = (int16_t)dealt0[i];
+        sp.nodes[i].nlive = 52 - g.nboard - __builtin_popcountll(dm[i]);
+        // variants: 5-card boards one; turn subgames one per dealt card, 52 =
+        // none; flop subgames 0 = none, 1 + t = turn card t, 53 + 52 t + r =
+        // turn t then river r
+        int var = 0;
+        if (g.nboard == 4) var = dealt[i] < 0 ? 52 : dealt[i];
+        else if (g.nboard == 3) var = dealt[i] < 0 ? 0 : (dealt0[i] < 0 ? 1 + dealt[i] : 53 + 52 * dealt0[i] + dealt[i]);
+        sp.nodes[i].var = var;
+        // a showdown needs all five board cards
+        if (g.nodes[i].type == MTT_NODE_SHOWDOWN && g.nboard + __builtin_popcountll(dm[i]) != 5) {
+            sp.status = MTT_ERR_INVALID;
+            return;
+        }
         // a depth-limit leaf stands for the river deal, so none sits below one
         if (g.nodes[i].type == MTT_NODE_LEAF && dealt[i] >= 0) { sp.status = MTT_ERR_INVALID; return; }
     }
     // tables
     const int vsize = tab_variant_bytes(H[0], H[1]);
-    const int nvar = g.nboard == 5 ? 1 : 53;
+    const int nvar = g.nboard == 5 ? 1 : (g.nboard == 4 ? 53 : 53 + 52 * 52);
     sp.tab.assign((size_t)vsize * nvar, 0);
     if (g.nboard == 5) {
         build_variant(g.board, 5, -1, H, cards, combos, sp.tab.data());
+    } else if (g.nboard == 3) {
+        // the variants some terminal uses, built on host threads
+        std::vector<char> used(nvar, 0);
+        for (int i = 0; i < nn; ++i)
+            if (g.nodes[i].type == MTT_NODE_FOLD || g.nodes[i].type == MTT_NODE_SHOWDOWN) used[sp.nodes[i].var] = 1;
+        std::vector<int> todo;
+        for (int v = 0; v < nvar; ++v) if (used[v]) todo.push_back(v);
+        auto build = [&](int v) {
+            uint8_t bd[5] = {g.board[0], g.board[1], g.board[2], 0, 0};
+            uint8_t* dst = sp.tab.data() + (size_t)vsize * v;
+            if (v == 0) {
+                build_variant(bd, 3, -1, H, cards, combos, dst);
+            } else if (v < 53) {
+                build_variant(bd, 3, v - 1, H, cards, combos, dst);
+            } else {
+                bd[3] = (uint8_t)((v - 53) / 52);
+                build_variant(bd, 4, (v - 53) % 52, H, cards, combos, dst);
+            }
+        };
+        const int nthr = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthr; ++t)
+            th.emplace_back([&, t]() { for (size_t k = t; k < todo.size(); k += nthr) build(todo[k]); });
+        for (auto& x : th) x.join();
     } else {
         for (int c = 0; c < 52; ++c) {
             if ((bm >> c) & 1ull) continue;
@@ -203,6 +260,7 @@ static void pack_one(const mtt_subgame& g, SubPack& sp) {
     d.tab_vsize = vsize;
     d.n_live = 52 - g.nboard;
     d.river = g.nboard == 5 ? 1 : 0;
+    d.var_none = g.nboard == 5 ? 0 : (g.nboard == 4 ? 52 : 0);
     d.pot = g.nodes[0].pot_size;
 }
 

@@ -26,7 +26,7 @@ struct BState {
     int raises;        // raises made after the first bet of this street
     bool bet_open;     // a bet is live this street
     bool first_checked;
-    int street;        // 4 turn, 5 river
+    int street;        // 3 flop, 4 turn, 5 river
 };
 
 struct Pending {
@@ -43,7 +43,8 @@ int build_tree(const mtt_tree_spec& sp, const uint8_t* /*board*/, std::vector<mt
                int rows[2], int* max_depth) {
     if (!(sp.pot > 0.0f) || sp.stack < 0.0f || sp.n_bet_sizes < 0 || sp.n_bet_sizes > MTT_MAX_SIZES ||
         sp.n_raise_sizes < 0 || sp.n_raise_sizes > MTT_MAX_SIZES || sp.raise_cap < 0 ||
-        (sp.street != 4 && sp.street != 5) || (sp.river_leaves && sp.street != 4))
+        sp.street < 3 || sp.street > 5 || (sp.river_leaves && sp.street != 4) || (sp.river_runout && sp.street == 5) ||
+        (sp.river_leaves && sp.river_runout))
         return MTT_ERR_INVALID;
     for (int i = 0; i < sp.n_bet_sizes; ++i) if (!(sp.bet_sizes[i] > 0.0f)) return MTT_ERR_INVALID;
     for (int i = 0; i < sp.n_raise_sizes; ++i) if (!(sp.raise_sizes[i] > 0.0f)) return MTT_ERR_INVALID;
@@ -206,73 +207,81 @@ int build_tree(const mtt_tree_spec& sp, const uint8_t* /*board*/, std::vector<mt
     return MTT_OK;
 }
 
-// Board-aware wrapper: expands every river chance node into one child per
-// card not on the 4-card board, each followed by a river betting round (or a
-// showdown when a player is all-in).  River subtrees are appended
-// breadth-first per chance node, keeping children contiguous and after their
-// parent.
+// Board-aware wrapper.  Turn trees (street 4, 4-card board) and flop trees
+// (street 3, 3-card board): every chance node gets one child per card not on
+// the board and not dealt above it.  Each child is followed by the next
+// street's betting round, grafted from a template built at the chance node's
+// commitments, or by showdowns when a player is all-in or the river is a
+// runout.  Flop trees always run the river out (flop and turn betting, then
+// the river dealt to showdowns, as the reference's multistreet solver);
+// turn trees do so with river_runout.  Subtrees are appended breadth-first
+// per chance node, keeping children contiguous and after their parent.
 int build_tree_board(const mtt_tree_spec& sp, const uint8_t* board, int nboard, std::vector<mtt_node>& out,
                      int rows[2], int* max_depth) {
     if (sp.street == 5) {
         if (nboard != 5 && nboard != 0) return MTT_ERR_INVALID;
         return build_tree(sp, board, out, rows, max_depth);
     }
-    if (nboard != 4) return MTT_ERR_INVALID;
-    std::vector<mtt_node> turn;
+    if (nboard != sp.street) return MTT_ERR_INVALID;
     int trows[2], tdepth = 0;
-    MTT_TRY(build_tree(sp, board, turn, trows, &tdepth));
+    MTT_TRY(build_tree(sp, board, out, trows, &tdepth));
     uint64_t bm = 0;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < nboard; ++k) {
         if (board[k] > 51 || ((bm >> board[k]) & 1ull)) return MTT_ERR_INVALID;
         bm |= 1ull << board[k];
     }
-    std::vector<int> river_cards;
-    for (int c = 0; c < 52; ++c) if (!((bm >> c) & 1ull)) river_cards.push_back(c);
-
-    // river template (street 5) for each chance node's state, built lazily
-    out = turn;
     rows[0] = trows[0];
     rows[1] = trows[1];
     int maxd = tdepth;
+    std::vector<uint64_t> above(out.size(), 0ull);   // cards dealt above each node
     // BFS over chance nodes in index order; appending keeps parents first.
     for (size_t i = 0; i < out.size(); ++i) {
         if (out[i].type != MTT_NODE_CHANCE) continue;
+        const uint64_t dm = above[i];
+        const int next = sp.street + __builtin_popcountll(dm) + 1;   // street of the round after this deal
         const float c0 = out[i].committed[0], c1 = out[i].committed[1];
         const int cdepth = out[i].depth;
         const float behind = out[i].reserved;
         out[i].reserved = 0.0f;
         const bool all_in = behind <= 0.0f;
+        const bool runout = next == 5 && (sp.street == 3 || sp.river_runout);
+        std::vector<int> cards;
+        for (int c = 0; c < 52; ++c) if (!(((bm | dm) >> c) & 1ull)) cards.push_back(c);
         const int first = (int)out.size();
         out[i].children_offset = first;
-        out[i].num_actions = (uint8_t)river_cards.size();
-        for (size_t k = 0; k < river_cards.size(); ++k) {
+        out[i].num_actions = (uint8_t)cards.size();
+        for (size_t k = 0; k < cards.size(); ++k) {
             mtt_node n{};
-            n.turn_idx = (int16_t)river_cards[k];
+            n.turn_idx = (int16_t)cards[k];
             n.depth = (int16_t)(cdepth + 1);
             out.push_back(n);
+            above.push_back(dm | (1ull << cards[k]));
         }
-        // river subtree template from this state
+        // the next round from this state (none for showdowns or a further deal)
         std::vector<mtt_node> rt;
         int rrows[2] = {0, 0}, rdepth = 0;
-        if (!all_in) {
+        const bool showdowns = next == 5 && (all_in || runout);
+        if (!showdowns && !all_in) {
             mtt_tree_spec rs = sp;
-            rs.street = 5;
-            // the river round starts from the chance node's commitments:
-            // express them through a pot/stack pair with the same remaining stacks
-            BState dummy{};
-            (void)dummy;
+            rs.street = next;
+            rs.river_leaves = 0;
+            rs.river_runout = runout || sp.street == 3;
+            // the round starts from the chance node's commitments: express
+            // them through a pot/stack pair with the same remaining stacks
             rs.pot = c0 + c1;
             rs.stack = behind;
             MTT_TRY(build_tree(rs, nullptr, rt, rrows, &rdepth));
         }
-        for (size_t k = 0; k < river_cards.size(); ++k) {
+        for (size_t k = 0; k < cards.size(); ++k) {
             const int ch = first + (int)k;
-            if (all_in) {
-                out[ch].type = MTT_NODE_SHOWDOWN;
-                out[ch].active_mask = 3;
+            if (showdowns || all_in) {
+                // all-in before the river: a further deal; else showdowns
+                out[ch].type = showdowns ? MTT_NODE_SHOWDOWN : MTT_NODE_CHANCE;
+                out[ch].active_mask = showdowns ? 3 : 0;
                 out[ch].pot_size = c0 + c1;
                 out[ch].committed[0] = c0;
                 out[ch].committed[1] = c1;
+                out[ch].reserved = 0.0f;
                 maxd = std::max(maxd, (int)out[ch].depth);
                 continue;
             }
@@ -285,16 +294,16 @@ int build_tree_board(const mtt_tree_spec& sp, const uint8_t* board, int nboard, 
                     n.infoset_offset += rows[n.player];
                 }
                 n.depth = (int16_t)(rt[j].depth + cdepth + 1);
-                n.turn_idx = (int16_t)(j == 0 ? river_cards[k] : -1);
+                n.turn_idx = (int16_t)(j == 0 ? cards[k] : -1);
                 maxd = std::max(maxd, (int)n.depth);
                 if (j == 0) out[ch] = n;
-                else out.push_back(n);
+                else { out.push_back(n); above.push_back(above[ch]); }
             }
             rows[0] += rrows[0];
             rows[1] += rrows[1];
         }
     }
-    // commitments inside river subtrees were expressed relative to rs.pot/2;
+    // commitments inside grafted rounds were expressed relative to rs.pot/2;
     // the builder put c = rs.pot/2 + bets for BOTH players, which equals the
     // true commitments only when c0 == c1 at the chance node (always true:
     // a round closes with equal commitments).

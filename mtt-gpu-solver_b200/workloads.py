@@ -137,3 +137,24 @@ def turn_dcfr(seed=1, n_hands=None):
         g[f"combos{p}"] = c.astype(np.uint16)
         g[f"range{p}"] = (r / r.sum()).astype(np.float32)
     return g
+
+
+def flop_runout(seed=6, n_hands=None, pot=100.0, stack=150.0, bet_sizes=(0.5, 1.0), raise_cap=1, alpha=0.3):
+    """A heads-up flop subgame with the reference's multistreet structure
+    (honest_multistreet_solver.cu:97-104,205-219): flop betting, 49 turn
+    cards, turn betting, then the river run out to showdowns.  A seeded
+    3-card flop; each player's range is a 1,326-entry Dirichlet(alpha)
+    weight vector with flop-blocked combos removed (or n_hands of the live
+    combos)."""
+    rng = np.random.default_rng(seed)
+    board = draw_board(rng, 3)
+    live = live_combos(board)
+    nodes, rows, _ = build_tree(pot, stack, list(bet_sizes), raise_cap=raise_cap, street=3, board=board)
+    g = {"nodes": nodes, "rows": rows, "board": board, "pot": float(pot)}
+    for p in (0, 1):
+        w = rng.dirichlet(np.full(1326, alpha))
+        c = live if n_hands is None else np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
+        r = w[c.astype(np.int64)]
+        g[f"combos{p}"] = c.astype(np.uint16)
+        g[f"range{p}"] = (r / r.sum()).astype(np.float32)
+    return g

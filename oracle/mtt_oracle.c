@@ -271,19 +271,28 @@ typedef struct orc_ctx {
     const orc_game* g;
     int n;
     int* parent;
-    int* dealt;          /* card dealt by the nearest chance ancestor, -1 if none */
+    uint64_t* dmask;     /* cards dealt at and above each node (chance children carry their card) */
+    int* sidx;           /* showdown nodes: row of score[] for the node's 5-card board, else -1 */
     uint64_t* hmask[2];  /* per hand card mask */
-    uint32_t* score[2];  /* [53][H_p]: score on board + dealt card (index 52 = no deal) */
-    int n_live;          /* cards not on the board */
+    uint32_t* score[2];  /* [n_boards][H_p]: score on each distinct showdown board */
+    int n_boards;
 } orc_ctx;
+
+static int popc64(uint64_t x) { int k = 0; while (x) { x &= x - 1; ++k; } return k; }
+
+/* Cards that a chance node can deal: not on the board, not dealt above. */
+static int orc_nlive(const orc_ctx* c, int node) {
+    return 52 - c->g->nboard - popc64(c->dmask[node]);
+}
 
 static int orc_ctx_init(orc_ctx* c, const orc_game* g) {
     memset(c, 0, sizeof(*c));
     c->g = g; c->n = g->n_nodes;
-    if (g->nboard != 5 && g->nboard != 4) return MTT_ERR_INVALID;
+    if (g->nboard < 3 || g->nboard > 5) return MTT_ERR_INVALID;
     c->parent = (int*)malloc(sizeof(int) * (size_t)c->n);
-    c->dealt = (int*)malloc(sizeof(int) * (size_t)c->n);
-    for (int i = 0; i < c->n; ++i) { c->parent[i] = -1; c->dealt[i] = -1; }
+    c->dmask = (uint64_t*)calloc((size_t)c->n, sizeof(uint64_t));
+    c->sidx = (int*)malloc(sizeof(int) * (size_t)c->n);
+    for (int i = 0; i < c->n; ++i) { c->parent[i] = -1; c->sidx[i] = -1; }
     for (int i = 0; i < c->n; ++i) {
         const mtt_node* nd = &g->nodes[i];
         if (nd->type == MTT_NODE_DECISION || nd->type == MTT_NODE_CHANCE)
@@ -292,36 +301,48 @@ static int orc_ctx_init(orc_ctx* c, const orc_game* g) {
     for (int i = 0; i < c->n; ++i) {   /* BFS order: parents first */
         int p = c->parent[i];
         if (p < 0) continue;
-        if (g->nodes[p].type == MTT_NODE_CHANCE) c->dealt[i] = g->nodes[i].turn_idx;
-        else c->dealt[i] = c->dealt[p];
+        c->dmask[i] = c->dmask[p];
+        if (g->nodes[p].type == MTT_NODE_CHANCE) c->dmask[i] |= 1ull << g->nodes[i].turn_idx;
     }
-    uint64_t bm = 0;
-    for (int k = 0; k < g->nboard; ++k) bm |= 1ull << g->board[k];
-    c->n_live = 52 - g->nboard;
+    /* distinct showdown boards (open addressing on the dealt-card mask) */
+    const int tsize = 1 << 14;
+    uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * tsize);
+    int* vals = (int*)malloc(sizeof(int) * tsize);
+    for (int k = 0; k < tsize; ++k) vals[k] = -1;
+    uint64_t* masks = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)c->n);
+    for (int i = 0; i < c->n; ++i) {
+        if (g->nodes[i].type != MTT_NODE_SHOWDOWN) continue;
+        uint64_t m = c->dmask[i];
+        unsigned hsh = (unsigned)((m * 0x9E3779B97F4A7C15ull) >> 50) & (tsize - 1);
+        while (vals[hsh] >= 0 && keys[hsh] != m) hsh = (hsh + 1) & (tsize - 1);
+        if (vals[hsh] < 0) { keys[hsh] = m; vals[hsh] = c->n_boards; masks[c->n_boards++] = m; }
+        c->sidx[i] = vals[hsh];
+    }
+    free(keys); free(vals);
     for (int p = 0; p < 2; ++p) {
         int H = g->H[p];
         c->hmask[p] = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(H > 0 ? H : 1));
-        c->score[p] = (uint32_t*)malloc(sizeof(uint32_t) * 53 * (size_t)(H > 0 ? H : 1));
+        c->score[p] = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(c->n_boards > 0 ? c->n_boards : 1) *
+                                        (size_t)(H > 0 ? H : 1));
         for (int h = 0; h < H; ++h)
             c->hmask[p][h] = (1ull << g->cards[p][2 * h]) | (1ull << g->cards[p][2 * h + 1]);
-        for (int d = 0; d < 53; ++d) {
-            int dc = d == 52 ? -1 : d;
-            if (g->nboard == 5 && dc != -1) continue;
-            if (g->nboard == 4 && (dc == -1 || ((bm >> dc) & 1))) continue;
+        for (int b = 0; b < c->n_boards; ++b) {
+            uint8_t c7[7];
+            int k = 0;
+            for (; k < g->nboard; ++k) c7[k] = g->board[k];
+            for (int x = 0; x < 52 && k < 5; ++x) if ((masks[b] >> x) & 1ull) c7[k++] = (uint8_t)x;
             for (int h = 0; h < H; ++h) {
-                uint8_t c7[7];
-                for (int k = 0; k < g->nboard; ++k) c7[k] = g->board[k];
-                if (g->nboard == 4) c7[4] = (uint8_t)dc;
                 c7[5] = g->cards[p][2 * h]; c7[6] = g->cards[p][2 * h + 1];
-                c->score[p][(size_t)d * H + h] = orc_score7(c7);
+                c->score[p][(size_t)b * H + h] = orc_score7(c7);
             }
         }
     }
+    free(masks);
     return MTT_OK;
 }
 
 static void orc_ctx_free(orc_ctx* c) {
-    free(c->parent); free(c->dealt);
+    free(c->parent); free(c->dmask); free(c->sidx);
     for (int p = 0; p < 2; ++p) { free(c->hmask[p]); free(c->score[p]); }
 }
 
@@ -332,8 +353,7 @@ static void orc_terminal_values(const orc_ctx* c, int node, int q, const double*
     const orc_game* g = c->g;
     const mtt_node* nd = &g->nodes[node];
     int o = 1 - q, Hq = g->H[q], Ho = g->H[o];
-    int dealt = c->dealt[node];
-    uint64_t dm = dealt >= 0 ? (1ull << dealt) : 0;
+    uint64_t dm = c->dmask[node];   /* cards dealt above: hands holding one are blocked */
     if (nd->type == MTT_NODE_FOLD) {
         int winner = (nd->active_mask == 1) ? 0 : 1;                       /* :135 */
         double payoff = (q == winner) ? (double)nd->pot_size - (double)nd->committed[q]
@@ -342,7 +362,7 @@ static void orc_terminal_values(const orc_ctx* c, int node, int q, const double*
         for (int j = 0; j < Ho; ++j) tot += ro[j];
         for (int h = 0; h < Hq; ++h) {
             double m;
-            if (c->hmask[q][h] & dm) { out[h] = 0.0; continue; }   /* blocked by the dealt card */
+            if (c->hmask[q][h] & dm) { out[h] = 0.0; continue; }   /* blocked by a dealt card */
             if (sem == ORC_SEM_REFERENCE) m = tot;
             else {
                 m = 0.0;
@@ -354,9 +374,8 @@ static void orc_terminal_values(const orc_ctx* c, int node, int q, const double*
         return;
     }
     /* showdown: honest:170-195 */
-    int d = (g->nboard == 5) ? 52 : dealt;
-    const uint32_t* sq = c->score[q] + (size_t)d * Hq;
-    const uint32_t* so = c->score[o] + (size_t)d * Ho;
+    const uint32_t* sq = c->score[q] + (size_t)c->sidx[node] * Hq;
+    const uint32_t* so = c->score[o] + (size_t)c->sidx[node] * Ho;
     double gain = (double)nd->pot_size - (double)nd->committed[q];
     double loss = -(double)nd->committed[q];
     double tie = 0.5 * (double)nd->pot_size - (double)nd->committed[q];
@@ -404,7 +423,6 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
     int Hmax = H[0] > H[1] ? H[0] : H[1];
     double* ro = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
     double* tv = (double*)malloc(sizeof(double) * (size_t)(Hmax + 1));
-    float chance_div = (prm->semantics == ORC_SEM_REFERENCE) ? (float)(c.n_live - 2) : (float)(c.n_live - 4);
 
     /* Simultaneous updates (the reference kernels: one forward and one
      * backward sweep update both players) or alternating updates (CFR+ as
@@ -500,6 +518,7 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
                     }
                 }
             } else if (nd->type == MTT_NODE_CHANCE) {                                /* :205-219 */
+                const float chance_div = (float)(orc_nlive(&c, i) - (prm->semantics == ORC_SEM_REFERENCE ? 2 : 4));
                 for (int p = 0; p < 2; ++p) {
                     if (!((upd >> p) & 1)) continue;
                     for (int h = 0; h < H[p]; ++h) {
@@ -509,7 +528,7 @@ int orc_cfr_solve(const orc_game* g, const orc_cfr_params* prm,
                             if (c.hmask[p][h] & (1ull << g->nodes[ch].turn_idx)) continue;
                             acc += cfv[p][(size_t)ch * H[p] + h];
                         }
-                        cfv[p][(size_t)i * H[p] + h] = acc / chance_div;
+                        cfv[p][(size_t)i * H[p] + h] = acc / chance_div;   /* N-2 or N-4, N per node */
                     }
                 }
             }
@@ -599,7 +618,7 @@ static int orc_values_fp64(const orc_game* g, const double* pol0, const double* 
                 ev[o][(size_t)i * H[o] + h] = se;
             }
         } else if (nd->type == MTT_NODE_CHANCE) {
-            double div = (double)(c.n_live - 4);
+            double div = (double)(orc_nlive(&c, i) - 4);
             for (int p = 0; p < 2; ++p)
                 for (int h = 0; h < H[p]; ++h) {
                     double sb = 0.0, se = 0.0;

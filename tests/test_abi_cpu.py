@@ -131,3 +131,30 @@ def test_turn_tree_with_river_leaves(mtt):
     assert int(np.sum(full["type"] == mtt.NODE_CHANCE)) == len(leaves) + int(np.sum(lim["type"] == mtt.NODE_CHANCE))
     with pytest.raises(mtt.MttError):
         mtt.build_tree(100.0, 150.0, [0.5], street=5, river_leaves=True)
+
+
+def test_flop_tree_turn_chance_and_river_runout(mtt):
+    """Flop trees: flop betting, a 49-card turn chance layer, turn betting,
+    then a 48-card river chance layer straight to showdowns; every showdown
+    sits below both deals."""
+    board = [3, 17, 42]
+    nodes, rows, depth = mtt.build_tree(100.0, 150.0, [0.5, 1.0], raise_cap=1, street=3, board=board)
+    assert mtt.validate_tree(nodes, rows) == 0
+    n = len(nodes)
+    parent = np.full(n, -1)
+    for i, nd in enumerate(nodes):
+        if nd["type"] in (mtt.NODE_DECISION, mtt.NODE_CHANCE):
+            parent[nd["children_offset"]:nd["children_offset"] + nd["num_actions"]] = i
+    deals = np.zeros(n, int)
+    for i in range(1, n):
+        deals[i] = deals[parent[i]] + (nodes[parent[i]]["type"] == mtt.NODE_CHANCE)
+    chance = nodes["type"] == mtt.NODE_CHANCE
+    assert set(nodes["num_actions"][chance & (deals == 0)]) == {49}
+    assert set(nodes["num_actions"][chance & (deals == 1)]) == {48}
+    assert np.all(deals[nodes["type"] == mtt.NODE_SHOWDOWN] == 2)
+    # no river betting: every child of a river chance node is a showdown
+    for i in np.nonzero(chance & (deals == 1))[0]:
+        c0 = nodes[i]["children_offset"]
+        assert np.all(nodes["type"][c0:c0 + nodes[i]["num_actions"]] == mtt.NODE_SHOWDOWN)
+    with pytest.raises(mtt.MttError):
+        mtt.build_tree(100.0, 150.0, [0.5], street=3, board=[3, 17, 42, 5])

@@ -103,8 +103,8 @@ def test_graph_replay_matches_direct(mtt, wl, cuda):
     assert np.array_equal(s1["S0"], s2["S0"]) and np.array_equal(s1["R1"], s2["R1"])
 
 
-@pytest.mark.parametrize("algo", [0, 1])
-def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda, algo):
+@pytest.mark.parametrize("algo,sem,alternate", [(0, 0, 1), (1, 0, 1), (0, 1, 0)])
+def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda, algo, sem, alternate):
     rng = np.random.default_rng(21)
     board = [int(c) for c in rng.choice(52, size=4, replace=False)]
     nodes, rows, _ = mtt.build_tree(60, 100, [0.75], raise_cap=1, street=4, board=board)
@@ -114,8 +114,8 @@ def test_turn_subgame_with_river_chance_vs_oracle(mtt, orc, cuda, algo):
     sub = {"nodes": nodes, "rows": rows, "board": board, "combos0": c0, "combos1": c1,
            "range0": rng.dirichlet(np.full(40, 0.3)).astype(np.float32),
            "range1": rng.dirichlet(np.full(36, 0.3)).astype(np.float32), "pot": 60.0}
-    res, reads = _solve_gpu(mtt, [sub], iters=3, algo=algo, threads=128)
-    o = orc.cfr_solve(sub, 3, algo=algo, alternate=1)
+    res, reads = _solve_gpu(mtt, [sub], iters=3, algo=algo, semantics=sem, alternate=alternate, threads=128)
+    o = orc.cfr_solve(sub, 3, algo=algo, semantics=sem, alternate=alternate)
     _compare(sub, o, reads[0])
     br = orc.best_response(sub, reads[0]["S0"], reads[0]["S1"])
     assert np.allclose(res[0], br, rtol=1e-8, atol=1e-9)
@@ -202,3 +202,38 @@ def test_kernel_profile_reports_each_kernel_class(mtt, wl, cuda):
     assert np.array_equal(r1, b2.results())
     b.close()
     b2.close()
+
+
+@pytest.mark.parametrize("algo,sem,alternate", [(0, 0, 1), (1, 0, 1), (0, 1, 0), (0, 0, 0)])
+def test_flop_subgame_turn_chance_and_river_runout_vs_oracle(mtt, wl, orc, cuda, algo, sem, alternate):
+    """Two chance layers (49 turn cards, then 48 river cards run out to
+    showdowns): table variants per (turn, river) board and chance divisors
+    per node, against the oracle's dense showdowns."""
+    sub = wl.flop_runout(seed=8, n_hands=36, stack=100.0, bet_sizes=(1.0,), raise_cap=0)
+    kinds = np.bincount(sub["nodes"]["type"], minlength=4)
+    assert kinds[3] > 49                     # turn chance nodes and the river chance nodes below them
+    res, reads = _solve_gpu(mtt, [sub], iters=3, algo=algo, semantics=sem, alternate=alternate, threads=128)
+    o = orc.cfr_solve(sub, 3, algo=algo, semantics=sem, alternate=alternate)
+    _compare(sub, o, reads[0])
+    br = orc.best_response(sub, reads[0]["S0"], reads[0]["S1"])
+    assert np.allclose(res[0], br, rtol=1e-8, atol=1e-9)
+
+
+def test_flop_subgame_full_ranges_converges(mtt, wl, cuda):
+    """Full flop ranges (1,176 live combos), 2 bet sizes + all-in, one raise:
+    exploitability falls with iterations, and graph replay equals direct
+    launches."""
+    sub = wl.flop_runout(seed=9)
+    expl = []
+    for iters in (20, 200):
+        res, _ = _solve_gpu(mtt, [sub], iters=iters, alternate=True, avg_power=2.0)
+        assert np.isfinite(res).all()
+        expl.append(res[0][5])
+    assert expl[1] < 0.5 * expl[0] and expl[1] < 0.02, expl
+    b = mtt.RiverBatch([sub])
+    p = mtt.solve_params(iters=10, alternate=True)
+    b.solve(p, graph=True)
+    r1 = b.results()
+    b.solve(p, graph=False)
+    assert np.array_equal(r1, b.results())
+    b.close()
