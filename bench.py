@@ -284,6 +284,19 @@ def other_configs(mtt, wl, stream):
     mtt.ev_dump(f4[:8])
     out["ev_dump_1755"] = {"ms": _event_ms(lambda: mtt.ev_dump(f4), stream),
                            "workload": "all 1,755 canonical flops, reference runout subsample (bit-exact dump)"}
+    # flop subgame: flop and turn betting, 49 turn cards, river run out
+    sub = wl.flop_runout(seed=9)
+    b = mtt.RiverBatch([sub])
+    pf3 = mtt.solve_params(iters=300, alternate=True, avg_power=2.0)
+    b.solve(pf3, graph=True)
+    t = _event_ms(lambda: b.solve(pf3, graph=True), stream)
+    out["flop_turn_runout"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
+                               "nodes": int(len(sub["nodes"])), "iter_bytes": int(b.info()["iter_bytes"]),
+                               "workload": "flop board, Dirichlet(0.3) ranges (1,176 live combos), pot 100, stack 150, "
+                                           "bets 50/100% + all-in, 1 raise on flop and turn, 49 turn cards then the "
+                                           "river run out (2,402 table variants), 300 alternating CFR+ iterations "
+                                           "+ FP64 best response"}
+    b.close()
     # depth-limited turn solve: leaf network trained on leaf samples of 64 full solves
     dlm = importlib.import_module("mtt-gpu-solver_b200.depthlimit")
     t0 = time.perf_counter()

@@ -226,7 +226,7 @@ typedef struct mtt_subgame {
     int32_t n_nodes;
     int32_t rows[2];
     uint8_t board[5];
-    int32_t nboard;               /* 5 river, 4 turn (tree has river chance nodes) */
+    int32_t nboard;               /* 5 river, 4 turn (river chance nodes), 3 flop (turn then river chance nodes) */
     int32_t H[2];
     const uint16_t* combos[2];
     const float* ranges[2];
