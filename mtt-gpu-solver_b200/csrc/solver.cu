@@ -1660,11 +1660,19 @@ static int grow(T** d, long long* cap, long long need, long long& total) {
 template <typename T, typename SubOf>
 static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv, const std::vector<char>* active,
                          SubOf sub_of, long long& total) {
-    std::vector<T> flat;
     L.off.assign(lv.size() + 1, 0);
+    if (!active) {   // every subgame: each level straight from its host vector
+        for (size_t d = 0; d < lv.size(); ++d) L.off[d + 1] = L.off[d] + (long long)lv[d].size();
+        MTT_TRY(grow(&L.d, &L.cap, L.off.back(), total));
+        for (size_t d = 0; d < lv.size(); ++d)
+            if (!lv[d].empty())
+                MTT_TRY_CUDA(cudaMemcpy(L.d + L.off[d], lv[d].data(), sizeof(T) * lv[d].size(), cudaMemcpyHostToDevice));
+        return MTT_OK;
+    }
+    std::vector<T> flat;
     for (size_t d = 0; d < lv.size(); ++d) {
         for (const T& x : lv[d])
-            if (!active || (*active)[sub_of(x)]) flat.push_back(x);
+            if ((*active)[sub_of(x)]) flat.push_back(x);
         L.off[d + 1] = (long long)flat.size();
     }
     MTT_TRY(grow(&L.d, &L.cap, (long long)flat.size(), total));
@@ -2172,13 +2180,16 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
     b->levels = levels;
     // FP64 best-response warp tasks, solver work items per level, terminal items
     HostLists& HL = b->host;
-    HL.bf.assign(levels, {}); HL.bb.assign(levels, {});
-    HL.fi.assign(levels, {}); HL.fsim.assign(levels, {}); HL.bsim.assign(levels, {});
-    for (int u = 0; u < 2; ++u) { HL.fal[u].assign(levels, {}); HL.bal[u].assign(levels, {}); }
+    auto init_lists = [levels](HostLists& L) {
+        L.bf.assign(levels, {}); L.bb.assign(levels, {});
+        L.fi.assign(levels, {}); L.fsim.assign(levels, {}); L.bsim.assign(levels, {});
+        for (int u = 0; u < 2; ++u) { L.fal[u].assign(levels, {}); L.bal[u].assign(levels, {}); }
+    };
     auto addT = [](std::vector<Task>& v, int node, int sub, int groups) {
         for (int g0 = 0; g0 < groups; g0 += 32) v.push_back(Task{node, sub, g0, 0});
     };
-    for (int i = 0; i < n; ++i) {
+    // one subgame's work items, appended to L (and its leaves to lv)
+    auto build_sub = [&](int i, HostLists& L, std::vector<LeafItem>& lv) {
         const SubDesc& d = b->desc[i];
         const long long HS = d.Hp0 + d.Hp1, nn = d.n_nodes;
         const int Hp[2] = {d.Hp0, d.Hp1}, Hh[2] = {d.H0, d.H1}, H4[2] = {d.Hp0 / 4, d.Hp1 / 4};
@@ -2200,11 +2211,11 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                 f.na = nd.na;
                 f.sub = i;
                 for (f.g0 = 0; f.g0 < f.h4; f.g0 += 32) {
-                    f.flags = FI_REACH; HL.fi[dp].push_back(f);
-                    f.flags = FI_REACH | FI_SUMS; HL.fsim[dp].push_back(f);
+                    f.flags = FI_REACH; L.fi[dp].push_back(f);
+                    f.flags = FI_REACH | FI_SUMS; L.fsim[dp].push_back(f);
                     // alternating pass u: the opponent's nodes pass reach down; the
                     // acting player's strategy sums are added by its backward items
-                    f.flags = FI_REACH; HL.fal[1 - p][dp].push_back(f);
+                    f.flags = FI_REACH; L.fal[1 - p][dp].push_back(f);
                 }
                 for (int q = 0; q < 2; ++q) {
                     BwdItem bw{};
@@ -2218,13 +2229,13 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     bw.hc = q == p ? f.reach_in : 0;
                     for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
                         bw.flags = q == p ? (BI_UPDATE | (q ? BI_NEG : 0)) : 0;
-                        HL.bsim[dp].push_back(bw);
+                        L.bsim[dp].push_back(bw);
                         if (q == p) bw.flags = BI_UPDATE | BI_SUMS;
-                        HL.bal[q][dp].push_back(bw);
+                        L.bal[q][dp].push_back(bw);
                     }
                 }
-                addT(HL.bf[dp], gn, i, H4[p]);
-                addT(HL.bb[dp], gn, i, Hmax);
+                addT(L.bf[dp], gn, i, H4[p]);
+                addT(L.bb[dp], gn, i, Hmax);
             } else if (nd.type == MTT_NODE_CHANCE) {
                 for (int p = 0; p < 2; ++p) {
                     FwdItem f{};
@@ -2238,9 +2249,9 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     f.first = (int)d.node_base + nd.first;
                     f.sub = i;
                     for (f.g0 = 0; f.g0 < f.h4; f.g0 += 32) {
-                        HL.fi[dp].push_back(f);
-                        HL.fsim[dp].push_back(f);
-                        HL.fal[1 - p][dp].push_back(f);     // pass u recomputes the other player's reach
+                        L.fi[dp].push_back(f);
+                        L.fsim[dp].push_back(f);
+                        L.fal[1 - p][dp].push_back(f);     // pass u recomputes the other player's reach
                     }
                     BwdItem bw{};
                     bw.child = cfv0 + (long long)nd.first * HS + off[p];
@@ -2254,12 +2265,12 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                     bw.div = (float)(nd.nlive - 4);
                     bw.sub = i;
                     for (bw.g0 = 0; bw.g0 < bw.h4; bw.g0 += 32) {
-                        HL.bsim[dp].push_back(bw);
-                        HL.bal[p][dp].push_back(bw);
+                        L.bsim[dp].push_back(bw);
+                        L.bal[p][dp].push_back(bw);
                     }
                 }
-                addT(HL.bf[dp], gn, i, Hmax);
-                addT(HL.bb[dp], gn, i, Hmax);
+                addT(L.bf[dp], gn, i, Hmax);
+                addT(L.bb[dp], gn, i, Hmax);
             } else if (nd.type == MTT_NODE_LEAF) {
                 LeafItem lf{};
                 for (int p = 0; p < 2; ++p) {
@@ -2271,14 +2282,14 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                 }
                 lf.pot = nd.pot;
                 lf.spr = nd.pot > 0.0f ? subs[i].nodes[k].reserved / nd.pot : 0.0f;
-                lf.row0 = LEAF_RIVERS * (int)b->h_leaves.size();
+                lf.row0 = 0;                          // set once the leaves are merged
                 lf.tab = d.tab_base;
                 lf.vsize = d.tab_vsize;
                 lf.sub = i;
                 for (int c = 0; c < 4; ++c) lf.board[c] = subs[i].board[c];
-                b->h_leaves.push_back(lf);
+                lv.push_back(lf);
             } else {
-                HL.terms.push_back(make_int2(gn, i));
+                L.terms.push_back(make_int2(gn, i));
                 TermItem t{};
                 for (int p = 0; p < 2; ++p) {
                     t.ro[p] = reach0 + src[p] * HS + off[p];
@@ -2292,14 +2303,53 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
                 t.c1 = nd.c1;
                 t.type_wmask = nd.type | (nd.wmask << 8);
                 t.sub = i;
-                HL.titems.push_back(t);
+                L.titems.push_back(t);
             }
         }
+    };
+    // subgames in contiguous chunks on host threads, merged in subgame order
+    // (the same lists, in the same order, as one thread would build)
+    const int nlt = std::max(1, std::min(n, std::min<int>((int)std::thread::hardware_concurrency(), 32)));
+    std::vector<HostLists> part(nlt);
+    std::vector<std::vector<LeafItem>> plv(nlt);
+    {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nlt; ++t)
+            th.emplace_back([&, t]() {
+                init_lists(part[t]);
+                const int lo = (int)((long long)n * t / nlt), hi = (int)((long long)n * (t + 1) / nlt);
+                for (int i = lo; i < hi; ++i) build_sub(i, part[t], plv[t]);
+                // terminals of one subgame and table variant are contiguous (terminal groups)
+                std::stable_sort(part[t].titems.begin(), part[t].titems.end(),
+                                 [](const TermItem& x, const TermItem& y) {
+                                     return x.sub != y.sub ? x.sub < y.sub : x.tab < y.tab;
+                                 });
+            });
+        for (auto& x : th) x.join();
     }
-    // terminals of one subgame and table variant are contiguous (terminal groups)
-    std::stable_sort(HL.titems.begin(), HL.titems.end(), [](const TermItem& x, const TermItem& y) {
-        return x.sub != y.sub ? x.sub < y.sub : x.tab < y.tab;
-    });
+    init_lists(HL);
+    auto merge = [&](auto get) {
+        size_t k = 0;
+        for (int t = 0; t < nlt; ++t) k += get(part[t]).size();
+        auto& dst = get(HL);
+        dst.reserve(k);
+        for (int t = 0; t < nlt; ++t) dst.insert(dst.end(), get(part[t]).begin(), get(part[t]).end());
+    };
+    for (int d = 0; d < levels; ++d) {
+        merge([d](HostLists& L) -> std::vector<Task>& { return L.bf[d]; });
+        merge([d](HostLists& L) -> std::vector<Task>& { return L.bb[d]; });
+        merge([d](HostLists& L) -> std::vector<FwdItem>& { return L.fi[d]; });
+        merge([d](HostLists& L) -> std::vector<FwdItem>& { return L.fsim[d]; });
+        merge([d](HostLists& L) -> std::vector<BwdItem>& { return L.bsim[d]; });
+        for (int u = 0; u < 2; ++u) {
+            merge([d, u](HostLists& L) -> std::vector<FwdItem>& { return L.fal[u][d]; });
+            merge([d, u](HostLists& L) -> std::vector<BwdItem>& { return L.bal[u][d]; });
+        }
+    }
+    merge([](HostLists& L) -> std::vector<TermItem>& { return L.titems; });
+    merge([](HostLists& L) -> std::vector<int2>& { return L.terms; });
+    for (int t = 0; t < nlt; ++t) b->h_leaves.insert(b->h_leaves.end(), plv[t].begin(), plv[t].end());
+    for (size_t k = 0; k < b->h_leaves.size(); ++k) b->h_leaves[k].row0 = LEAF_RIVERS * (int)k;
     long long total = 0;
     int s = MTT_OK;
     if (!s) s = dalloc(&b->d_desc, n, total);
