@@ -304,6 +304,11 @@ int mtt_batch_check(mtt_batch* b, void* stream);
 /* Kernels launched for this batch since it was created; a graph replay counts
  * every kernel node it runs. No reference counterpart (instrumentation). */
 int mtt_batch_launch_count(mtt_batch* b, int64_t* launches);
+/* Batches allocate device memory from a library-owned stream-ordered pool
+ * per device that keeps what destroyed batches free, so the next batch of a
+ * similar size allocates without mapping new pages.  mtt_trim_pool waits for
+ * the current device and returns the kept memory to the driver. */
+int mtt_trim_pool(void);
 /* Depth-limit leaves (MTT_NODE_LEAF, turn subgames): every pass of every
  * iteration values them by the leaf network `net` (whose batch capacity must
  * hold 48 rows per leaf of the batch) on both players' current reach, per

@@ -221,6 +221,12 @@ def solve_params(iters=1000, algo=ALGO_CFRPLUS, alpha=1.5, beta=0.0, gamma=2.0, 
     return p
 
 
+def trim_pool():
+    """Returns the device memory that destroyed batches left in the library's
+    pool to the driver (the pool keeps it for the next batch otherwise)."""
+    check("mtt_trim_pool", lib().mtt_trim_pool())
+
+
 class RiverBatch:
     """A batch of heads-up subgames resident on the current CUDA device.
 

@@ -237,3 +237,19 @@ def test_flop_subgame_full_ranges_converges(mtt, wl, cuda):
     b.solve(p, graph=False)
     assert np.array_equal(r1, b.results())
     b.close()
+
+
+def test_batches_reuse_pool_memory_and_trim(mtt, wl, cuda):
+    """A batch created where a destroyed one was (pool memory kept) solves
+    the same; trimming returns the memory and later batches still work."""
+    subs = wl.river_batch(n=12, seed=31, min_support=60, max_support=300, max_sizes=2)
+    p = mtt.solve_params(iters=20, alternate=True, threads=128)
+    out = []
+    for k in range(3):
+        b = mtt.RiverBatch(subs)
+        b.solve(p, graph=True)
+        out.append(b.results())
+        b.close()
+        if k == 1:
+            mtt.trim_pool()
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
