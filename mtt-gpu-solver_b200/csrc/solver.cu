@@ -1754,11 +1754,22 @@ static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, 
     L.n_terms = (int)tm.size();
     L.n_subs = (int)subs.size();
     // Terminal groups: runs of items with the same subgame and table variant
-    // (the host list is ordered that way), cut into chunks of TG_CHUNK.
+    // (the host list is ordered that way), cut into chunks.  A CTA walks its
+    // chunk's terminals one after another, so small batches (a single
+    // subgame, the few still above the exploitability gate) get short chunks
+    // and spread over the SMs: about 4 chunks per SM and CTA slot, TG_CHUNK
+    // at most.
+    int sm_count = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const long long slots = 4LL * 5 * std::max(sm_count, 1);   // 5 CTAs per SM
+    const int chunk = (int)std::max(1LL, std::min<long long>(TG_CHUNK, (long long)ti.size() / slots));
     std::vector<TermGroup> gr;
     for (int i = 0; i < (int)ti.size();) {
         int j = i + 1;
-        while (j < (int)ti.size() && j - i < TG_CHUNK && ti[j].sub == ti[i].sub && ti[j].tab == ti[i].tab) ++j;
+        while (j < (int)ti.size() && j - i < chunk && ti[j].sub == ti[i].sub && ti[j].tab == ti[i].tab) ++j;
         TermGroup g{};
         g.tab = ti[i].tab;
         g.first = i;
