@@ -74,6 +74,38 @@ def build(force=False, jobs=8, verbose_ptxas=False, quiet=False):
     return LIB
 
 
+DRIVERS = os.path.join(HERE, "drivers")
+BIN = os.path.join(HERE, "bin")
+CUDA_LIB = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
+
+
+def build_drivers(force=False, quiet=False):
+    """The command-line drivers (ev_dumper, preflop_gen, hu_solver,
+    multiway_solver): host C++ over the C ABI, linked to libmtt_b200.so next
+    to them (rpath $ORIGIN/..) into bin/."""
+    os.makedirs(BIN, exist_ok=True)
+    deps = glob.glob(os.path.join(DRIVERS, "*.h")) + [os.path.join(ROOT, "include", "mtt_b200.h"), LIB]
+    dep_mtime = max(os.path.getmtime(d) for d in deps if os.path.exists(d))
+    built = []
+    for src in sorted(glob.glob(os.path.join(DRIVERS, "*.cpp"))):
+        exe = os.path.join(BIN, os.path.splitext(os.path.basename(src))[0])
+        built.append(exe)
+        if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), dep_mtime):
+            continue
+        cmd = [NVCC] + CCBIN + ARCH + ["-O2", "-std=c++17", "-x", "c++", src, "-I" + os.path.join(ROOT, "include"),
+                                "-I" + DRIVERS, "-L" + HERE, "-lmtt_b200", "-L" + CUDA_LIB, "-lcudart",
+                                "-Xlinker", "--disable-new-dtags", "-Xlinker", "-rpath=$ORIGIN/..",
+                                "-Xlinker", "-rpath=" + CUDA_LIB, "-o", exe + ".tmp"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(f"[build] FAILED {' '.join(cmd)}\n{r.stdout}{r.stderr}\n")
+            raise RuntimeError(f"driver build failed: {os.path.basename(src)}")
+        if (r.stdout + r.stderr).strip() and not quiet:
+            sys.stderr.write(r.stdout + r.stderr)
+        shutil.move(exe + ".tmp", exe)
+    return built
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
@@ -81,3 +113,5 @@ if __name__ == "__main__":
     ap.add_argument("--ptxas", action="store_true", help="print -Xptxas -v (registers, spills, smem)")
     a = ap.parse_args()
     print(build(force=a.force, jobs=a.jobs, verbose_ptxas=a.ptxas))
+    for exe in build_drivers(force=a.force):
+        print(exe)

@@ -158,3 +158,20 @@ def test_flop_tree_turn_chance_and_river_runout(mtt):
         assert np.all(nodes["type"][c0:c0 + nodes[i]["num_actions"]] == mtt.NODE_SHOWDOWN)
     with pytest.raises(mtt.MttError):
         mtt.build_tree(100.0, 150.0, [0.5], street=3, board=[3, 17, 42, 5])
+
+
+def test_command_line_drivers_build_and_print_usage():
+    """The reference's executables (Makefile: ev_dumper, preflop_gen,
+    hu_solver, multiway_solver), built over the C ABI; --help needs no GPU."""
+    import importlib.util
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("mtt_build", os.path.join(root, "mtt-gpu-solver_b200", "build.py"))
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    exes = b.build_drivers(quiet=True)
+    assert sorted(os.path.basename(e) for e in exes) == ["ev_dumper", "hu_solver", "multiway_solver", "preflop_gen"]
+    for e in exes:
+        r = subprocess.run([e, "--help"], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 0 and r.stdout.startswith("usage: " + os.path.basename(e)), (e, r.stdout, r.stderr)
