@@ -346,6 +346,7 @@ def run_b200(args, rank, world, local):
     batch = mtt.RiverBatch(subs)
     threads = batch.autotune(p)
     p.threads = threads
+    sched = batch.schedule()       # autotuned: CTA size, hands per warp item, terminals per CTA
     info = batch.info()
 
     def step():
@@ -476,6 +477,7 @@ def run_b200(args, rank, world, local):
                                    f"+ FP64 exploitability, continued to <= {args.target * 100:g}% pot",
                        "subgames_per_gpu": args.subgames,
                        "iters": args.iters, "seed": args.seed, "cta_threads": threads,
+                       "schedule": sched,
                        "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (info["device_bytes"] / 1e9),
                        "parallelism": f"replicas x{world}"},
             "exploitability_pct_pot": {"median": float(np.median(expl) * 100), "max": float(np.max(expl) * 100),

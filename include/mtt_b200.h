@@ -330,9 +330,17 @@ int mtt_batch_set_leafnet(mtt_batch* b, mtt_leafnet* net, int32_t flags);
  * No reference counterpart (instrumentation). */
 int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
                              double* h_bytes, void* stream);
-/* Pick the CTA size by timing a few iterations of each candidate on this
- * batch; *threads receives the choice (also used when params.threads == 0). */
+/* Pick the schedule by timing a few iterations of every candidate on this
+ * batch: the sweep CTA size (64, 128, 256 threads), the hands per sweep warp
+ * item (128 or 256) and the terminals per terminal CTA at most (8 or 16);
+ * *threads receives the CTA size (also used when params.threads == 0), the
+ * rest stays set on the batch (mtt_batch_schedule).  Results do not depend on
+ * the schedule. */
 int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads);
+/* Set the schedule: threads 0 (256 unless tuned) or 64/128/256,
+ * hands_per_warp 128 or 256, term_chunk 1..16.  Rebuilds the work lists. */
+int mtt_batch_set_schedule(mtt_batch* b, int32_t threads, int32_t hands_per_warp, int32_t term_chunk);
+int mtt_batch_schedule(mtt_batch* b, int32_t* threads, int32_t* hands_per_warp, int32_t* term_chunk);
 int mtt_batch_destroy(mtt_batch* b);
 
 /* ------------------------------------------------------ leaf-net GEMM */

@@ -366,6 +366,18 @@ class RiverBatch:
         return {k: {"ms": float(ms[i]), "bytes": float(by[i])}
                 for i, k in enumerate(("k_fwd", "k_term", "k_bwd"))}
 
+    def set_schedule(self, threads=0, hands_per_warp=128, term_chunk=16):
+        """Sweep CTA size (0 = default), hands per sweep warp item (128 or
+        256) and terminals per terminal CTA at most (1..16)."""
+        check("mtt_batch_set_schedule", lib().mtt_batch_set_schedule(self._h, int(threads), int(hands_per_warp),
+                                                                     int(term_chunk)))
+
+    def schedule(self):
+        t, h, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check("mtt_batch_schedule", lib().mtt_batch_schedule(self._h, ctypes.byref(t), ctypes.byref(h),
+                                                             ctypes.byref(c)))
+        return {"threads": t.value, "hands_per_warp": h.value, "term_chunk": c.value}
+
     def autotune(self, params, stream=None):
         t = ctypes.c_int32()
         check("mtt_batch_autotune", lib().mtt_batch_autotune(self._h, ctypes.byref(params), _stream(stream),

@@ -117,6 +117,8 @@ def lib():
         "mtt_batch_kernel_profile": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
         "mtt_batch_set_leafnet": ([vp, vp, i32], ctypes.c_int),
         "mtt_trim_pool": ([], ctypes.c_int),
+        "mtt_batch_set_schedule": ([vp, i32, i32, i32], ctypes.c_int),
+        "mtt_batch_schedule": ([vp, vp, vp, vp], ctypes.c_int),
         "mtt_leafnet_capacity": ([vp, vp], ctypes.c_int),
         "mtt_batch_layout": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_ev_grad": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),

@@ -93,6 +93,7 @@ struct SolveDev {
     int* iter;          // device iteration counter, 1-based
     int* err;           // bit 0: a bounded wait for a bulk copy gave up
     int algo, semantics;
+    int span;           // float4 hand groups per sweep work item / 32 (hands per warp / 128)
 };
 
 #define HP(p) ((p) ? sd.Hp1 : sd.Hp0)
@@ -632,11 +633,7 @@ __device__ __forceinline__ void bwd_sum_fixed(const float4* __restrict__ qc, flo
 
 // Forward sweep of one level: regret matching, children's reach and/or
 // strategy sums (kernel_forward_sweep, honest_multistreet_solver.cu:88-126).
-__global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const FwdItem it = items[w];
+__device__ __forceinline__ void k_fwd_group(const SolveDev& a, const FwdItem& it, const int lane) {
     const float4* rp = reinterpret_cast<const float4*>(a.arena + it.reach_in);
     float4* ch = reinterpret_cast<float4*>(a.arena + it.child);
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -701,6 +698,19 @@ __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __res
                 Sb[(size_t)k * H4 + g] = sv;
             }
         }
+    }
+}
+
+// One warp per work item; the item covers span x 32 float4 hand groups.
+template <int SPAN>
+__global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n) return;
+    const FwdItem it = items[w];
+#pragma unroll
+    for (int s = 0; s < SPAN; ++s) {
+        if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
+        k_fwd_group(a, it, (threadIdx.x & 31) + 32 * s);
     }
 }
 
@@ -897,11 +907,7 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
 
 // Backward sweep of one level for the updated players: counterfactual values
 // and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
-__global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const BwdItem it = items[w];
+__device__ __forceinline__ void k_bwd_group(const SolveDev& a, const BwdItem& it, const int lane) {
     const float4* qc = reinterpret_cast<const float4*>(a.arena + it.child);
     float4* out = reinterpret_cast<float4*>(a.arena + it.self);
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -999,6 +1005,19 @@ __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __res
             }
             Rb[(size_t)k * H4 + g] = nr;
         }
+    }
+}
+
+// One warp per work item; the item covers span x 32 float4 hand groups.
+template <int SPAN>
+__global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n) return;
+    const BwdItem it = items[w];
+#pragma unroll
+    for (int s = 0; s < SPAN; ++s) {
+        if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
+        k_bwd_group(a, it, (threadIdx.x & 31) + 32 * s);
     }
 }
 
@@ -1231,11 +1250,7 @@ __global__ void k_ev_init(SolveDev a, int n_sub) {
 }
 
 // Forward level: children's reach under softmax strategies; chance items as k_fwd.
-__global__ void __launch_bounds__(256) k_ev_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const FwdItem it = items[w];
+__device__ __forceinline__ void k_ev_fwd_group(const SolveDev& a, const FwdItem& it, const int lane) {
     const float4* rp = reinterpret_cast<const float4*>(a.arena + it.reach_in);
     float4* ch = reinterpret_cast<float4*>(a.arena + it.child);
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -1264,13 +1279,22 @@ __global__ void __launch_bounds__(256) k_ev_fwd(SolveDev a, const FwdItem* __res
     for (int k = 0; k < A; ++k) ch[(size_t)k * HS4 + g] = mul4(r, softmax_at(Lb, H4, g, k, mx, den));
 }
 
+// One warp per work item; the item covers span x 32 float4 hand groups.
+template <int SPAN>
+__global__ void __launch_bounds__(256) k_ev_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n) return;
+    const FwdItem it = items[w];
+#pragma unroll
+    for (int s = 0; s < SPAN; ++s) {
+        if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
+        k_ev_fwd_group(a, it, (threadIdx.x & 31) + 32 * s);
+    }
+}
+
 // Backward level: values of both players; the acting player's items also
 // write the logit gradient.
-__global__ void __launch_bounds__(256) k_ev_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const BwdItem it = items[w];
+__device__ __forceinline__ void k_ev_bwd_group(const SolveDev& a, const BwdItem& it, const int lane) {
     const float4* qc = reinterpret_cast<const float4*>(a.arena + it.child);
     float4* out = reinterpret_cast<float4*>(a.arena + it.self);
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -1314,6 +1338,19 @@ __global__ void __launch_bounds__(256) k_ev_bwd(SolveDev a, const BwdItem* __res
         const float4 d = make_float4(__fsub_rn(qc[(size_t)k * HS4 + g].x, v.x), __fsub_rn(qc[(size_t)k * HS4 + g].y, v.y),
                                      __fsub_rn(qc[(size_t)k * HS4 + g].z, v.z), __fsub_rn(qc[(size_t)k * HS4 + g].w, v.w));
         Gb[(size_t)k * H4 + g] = mul4(mul4(sr, sg), d);
+    }
+}
+
+// One warp per work item; the item covers span x 32 float4 hand groups.
+template <int SPAN>
+__global__ void __launch_bounds__(256) k_ev_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n) return;
+    const BwdItem it = items[w];
+#pragma unroll
+    for (int s = 0; s < SPAN; ++s) {
+        if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
+        k_ev_bwd_group(a, it, (threadIdx.x & 31) + 32 * s);
     }
 }
 
@@ -1614,6 +1651,10 @@ struct mtt_batch {
     float *d_lx = nullptr, *d_ly = nullptr, *d_lm = nullptr, *d_lsd = nullptr;
     int leaf_sd_stride = 0;            // floats per (row, player) of d_lsd
     int leaf_smem = 0;                 // dynamic shared memory of k_leaf_showdown
+    // schedule (mtt_batch_set_schedule / the autotuner): 32 x span float4
+    // hand groups per sweep work item, at most tchunk terminals per CTA
+    int span = 1;
+    int tchunk = mtt::TG_CHUNK;
 };
 
 namespace mtt {
@@ -1702,11 +1743,11 @@ static int grow(T** d, long long* cap, long long need, long long& total) {
 
 // Upload the per-depth lists, keeping the entries whose subgame is active
 // (all when `active` is null).
-template <typename T, typename SubOf>
-static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv, const std::vector<char>* active,
-                         SubOf sub_of, long long& total) {
+template <typename T, typename Keep>
+static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv, bool all, Keep keep,
+                         long long& total) {
     L.off.assign(lv.size() + 1, 0);
-    if (!active) {   // every subgame: each level straight from its host vector
+    if (all) {   // every item: each level straight from its host vector
         for (size_t d = 0; d < lv.size(); ++d) L.off[d + 1] = L.off[d] + (long long)lv[d].size();
         MTT_TRY(grow(&L.d, &L.cap, L.off.back(), total));
         for (size_t d = 0; d < lv.size(); ++d)
@@ -1717,7 +1758,7 @@ static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv
     std::vector<T> flat;
     for (size_t d = 0; d < lv.size(); ++d) {
         for (const T& x : lv[d])
-            if ((*active)[sub_of(x)]) flat.push_back(x);
+            if (keep(x)) flat.push_back(x);
         L.off[d + 1] = (long long)flat.size();
     }
     MTT_TRY(grow(&L.d, &L.cap, (long long)flat.size(), total));
@@ -1727,18 +1768,22 @@ static int upload_levels(LevelLists<T>& L, const std::vector<std::vector<T>>& lv
 
 static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, long long& total) {
     const HostLists& H = b->host;
-    auto fsub = [](const FwdItem& x) { return x.sub; };
-    auto bsub = [](const BwdItem& x) { return x.sub; };
-    auto tsub = [](const Task& x) { return x.sub; };
-    MTT_TRY(upload_levels(L.f_init, H.fi, active, fsub, total));
-    MTT_TRY(upload_levels(L.f_sim, H.fsim, active, fsub, total));
-    MTT_TRY(upload_levels(L.b_sim, H.bsim, active, bsub, total));
+    // the host lists hold one item per 32 float4 groups; a span of k keeps
+    // every k-th (the kernels then walk 32 k groups per item)
+    const int span = b->span;
+    auto fkeep = [&](const FwdItem& x) { return (!active || (*active)[x.sub]) && (x.g0 / 32) % span == 0; };
+    auto bkeep = [&](const BwdItem& x) { return (!active || (*active)[x.sub]) && (x.g0 / 32) % span == 0; };
+    auto tkeep = [&](const Task& x) { return !active || (*active)[x.sub]; };
+    const bool all_sweep = !active && span == 1;
+    MTT_TRY(upload_levels(L.f_init, H.fi, all_sweep, fkeep, total));
+    MTT_TRY(upload_levels(L.f_sim, H.fsim, all_sweep, fkeep, total));
+    MTT_TRY(upload_levels(L.b_sim, H.bsim, all_sweep, bkeep, total));
     for (int u = 0; u < 2; ++u) {
-        MTT_TRY(upload_levels(L.f_alt[u], H.fal[u], active, fsub, total));
-        MTT_TRY(upload_levels(L.b_alt[u], H.bal[u], active, bsub, total));
+        MTT_TRY(upload_levels(L.f_alt[u], H.fal[u], all_sweep, fkeep, total));
+        MTT_TRY(upload_levels(L.b_alt[u], H.bal[u], all_sweep, bkeep, total));
     }
-    MTT_TRY(upload_levels(L.br_fwd, H.bf, active, tsub, total));
-    MTT_TRY(upload_levels(L.br_bwd, H.bb, active, tsub, total));
+    MTT_TRY(upload_levels(L.br_fwd, H.bf, !active, tkeep, total));
+    MTT_TRY(upload_levels(L.br_bwd, H.bb, !active, tkeep, total));
     std::vector<TermItem> ti;
     std::vector<int2> tm;
     std::vector<int> subs;
@@ -1765,7 +1810,7 @@ static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, 
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
     }
     const long long slots = 4LL * 5 * std::max(sm_count, 1);   // 5 CTAs per SM
-    const int chunk = (int)std::max(1LL, std::min<long long>(TG_CHUNK, (long long)ti.size() / slots));
+    const int chunk = (int)std::max(1LL, std::min<long long>(b->tchunk, (long long)ti.size() / slots));
     std::vector<TermGroup> gr;
     for (int i = 0; i < (int)ti.size();) {
         int j = i + 1;
@@ -1837,6 +1882,7 @@ static SolveDev dev_args(const mtt_batch* b, const mtt_solve_params& p) {
     a.desc = b->d_desc; a.nodes = b->d_nodes; a.tabs = b->d_tabs; a.hcards = b->d_hcards; a.ranges = b->d_ranges;
     a.arena = b->d_arena; a.R = b->d_R; a.S = b->d_S; a.darena = b->d_darena; a.results = b->d_results;
     a.iter_tab = b->d_iter_tab; a.iter = b->d_iter; a.err = b->d_err; a.algo = p.algo; a.semantics = p.semantics;
+    a.span = b->span;
     return a;
 }
 
@@ -1848,7 +1894,8 @@ static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelL
     for (int d = 0; d < b->levels; ++d) {
         const long long n = L.off[d + 1] - L.off[d];
         if (n == 0) continue;
-        k_fwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        if (a.span == 2) k_fwd<2><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        else k_fwd<1><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
         MTT_CHECK_LAUNCH();
         ++b->launches;
     }
@@ -1861,7 +1908,8 @@ static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelL
     for (int d = b->levels - 1; d >= 0; --d) {
         const long long n = L.off[d + 1] - L.off[d];
         if (n == 0) continue;
-        k_bwd<<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        if (a.span == 2) k_bwd<2><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        else k_bwd<1><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
         MTT_CHECK_LAUNCH();
         ++b->launches;
     }
@@ -2080,13 +2128,15 @@ static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, b
 // Compulsory bytes of one work item: every element it reads or writes,
 // counted once (the second read of a regret row hits L1).  g: float4 groups
 // the item's warp covers.
-static double fwd_item_bytes(const FwdItem& it) {
-    const double g = (double)std::min(32, it.h4 - it.g0), row = 16.0 * g, A = it.na;
+static double fwd_item_bytes(const FwdItem& it, int span) {
+    if ((it.g0 / 32) % span) return 0.0;   // covered by the item span groups before it
+    const double g = (double)std::min(32 * span, it.h4 - it.g0), row = 16.0 * g, A = it.na;
     if (it.flags & FI_CHANCE) return row * (1.0 + A) + 8.0 * g;       // reach, children, hand cards
     return row * (1.0 + A + ((it.flags & FI_REACH) ? A : 0.0) + ((it.flags & FI_SUMS) ? 2.0 * A : 0.0));
 }
-static double bwd_item_bytes(const BwdItem& it) {
-    const double g = (double)std::min(32, it.h4 - it.g0), row = 16.0 * g, A = it.na;
+static double bwd_item_bytes(const BwdItem& it, int span) {
+    if ((it.g0 / 32) % span) return 0.0;
+    const double g = (double)std::min(32 * span, it.h4 - it.g0), row = 16.0 * g, A = it.na;
     if (it.flags & BI_CHANCE) return row * (A + 1.0) + 8.0 * g;       // children, value, hand cards
     if (!(it.flags & BI_UPDATE)) return row * (A + 1.0);
     // regret rows read and written, children read, value written; sums: reach and S rows
@@ -2129,13 +2179,13 @@ extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* pr
         MTT_TRY_CUDA(cudaMemcpy(gr.data(), L.tgroups, sizeof(TermGroup) * gr.size(), cudaMemcpyDeviceToHost));
     if (p.alternate) {
         for (int u = 0; u < 2; ++u) {
-            for (const auto& lv : HL.fal[u]) for (const FwdItem& it : lv) bf += fwd_item_bytes(it);
-            for (const auto& lv : HL.bal[u]) for (const BwdItem& it : lv) bb += bwd_item_bytes(it);
+            for (const auto& lv : HL.fal[u]) for (const FwdItem& it : lv) bf += fwd_item_bytes(it, b->span);
+            for (const auto& lv : HL.bal[u]) for (const BwdItem& it : lv) bb += bwd_item_bytes(it, b->span);
             bt += term_launch_bytes(L, gr, HL.titems, 1 << u);
         }
     } else {
-        for (const auto& lv : HL.fsim) for (const FwdItem& it : lv) bf += fwd_item_bytes(it);
-        for (const auto& lv : HL.bsim) for (const BwdItem& it : lv) bb += bwd_item_bytes(it);
+        for (const auto& lv : HL.fsim) for (const FwdItem& it : lv) bf += fwd_item_bytes(it, b->span);
+        for (const auto& lv : HL.bsim) for (const BwdItem& it : lv) bb += bwd_item_bytes(it, b->span);
         bt += term_launch_bytes(L, gr, HL.titems, 3);
     }
     h_bytes[0] = bf; h_bytes[1] = bt; h_bytes[2] = bb;
@@ -2630,7 +2680,8 @@ extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const floa
     for (int d = 0; d < b->levels; ++d) {
         const long long n = L.f_init.off[d + 1] - L.f_init.off[d];
         if (n == 0) continue;
-        k_ev_fwd<<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.f_init.d + L.f_init.off[d], (int)n);
+        if (a.span == 2) k_ev_fwd<2><<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.f_init.d + L.f_init.off[d], (int)n);
+        else k_ev_fwd<1><<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.f_init.d + L.f_init.off[d], (int)n);
         MTT_CHECK_LAUNCH();
         ++b->launches;
     }
@@ -2638,7 +2689,8 @@ extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const floa
     for (int d = b->levels - 1; d >= 0; --d) {
         const long long n = L.b_sim.off[d + 1] - L.b_sim.off[d];
         if (n == 0) continue;
-        k_ev_bwd<<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.b_sim.d + L.b_sim.off[d], (int)n);
+        if (a.span == 2) k_ev_bwd<2><<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.b_sim.d + L.b_sim.off[d], (int)n);
+        else k_ev_bwd<1><<<(unsigned)((n + warps - 1) / warps), 256, 0, st>>>(a, L.b_sim.d + L.b_sim.off[d], (int)n);
         MTT_CHECK_LAUNCH();
         ++b->launches;
     }
@@ -2663,7 +2715,42 @@ extern "C" int mtt_batch_launch_count(mtt_batch* b, int64_t* launches) {
     return MTT_OK;
 }
 
+namespace mtt {
+// Switch the batch to `span` x 32 float4 groups per sweep item and at most
+// `chunk` terminals per CTA: the full work lists are rebuilt from the host
+// lists and the cached iteration graph is dropped.
+static int apply_schedule(mtt_batch* b, int span, int chunk) {
+    if (span == b->span && chunk == b->tchunk) return MTT_OK;
+    MTT_TRY_CUDA(cudaDeviceSynchronize());
+    b->span = span;
+    b->tchunk = chunk;
+    long long total = 0;
+    MTT_TRY(build_set(b, b->full, nullptr, total));
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    return MTT_OK;
+}
+}  // namespace mtt
+
+extern "C" int mtt_batch_set_schedule(mtt_batch* b, int32_t threads, int32_t hands_per_warp, int32_t term_chunk) {
+    using namespace mtt;
+    if (!b || (threads != 0 && threads != 64 && threads != 128 && threads != 256) ||
+        (hands_per_warp != 128 && hands_per_warp != 256) || term_chunk < 1 || term_chunk > TG_CHUNK)
+        return MTT_ERR_INVALID;
+    MTT_TRY(apply_schedule(b, hands_per_warp / 128, term_chunk));
+    b->tuned_threads = threads;
+    return MTT_OK;
+}
+
+extern "C" int mtt_batch_schedule(mtt_batch* b, int32_t* threads, int32_t* hands_per_warp, int32_t* term_chunk) {
+    if (!b) return MTT_ERR_INVALID;
+    if (threads) *threads = b->tuned_threads ? b->tuned_threads : 256;
+    if (hands_per_warp) *hands_per_warp = 128 * b->span;
+    if (term_chunk) *term_chunk = b->tchunk;
+    return MTT_OK;
+}
+
 extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads) {
+    using namespace mtt;
     if (!b) return MTT_ERR_INVALID;
     if (b->n_leaves && !b->leaf_ready) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
@@ -2672,29 +2759,36 @@ extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, voi
     p.iters = std::min(std::max(prm->iters, 1), 8);
     p.exploitability = 0;
     p.target_expl = 0.0f;
-    const int cands[3] = {64, 128, 256};
+    // every schedule: hands per warp item x terminals per CTA x sweep CTA size
+    const int spans[2] = {1, 2}, chunks[2] = {8, 16}, cands[3] = {64, 128, 256};
     float best_ms = 1e30f;
-    int best = 256;
+    int best_t = 256, best_span = b->span, best_chunk = b->tchunk;
     cudaEvent_t e0, e1;
     MTT_TRY_CUDA(cudaEventCreate(&e0));
     MTT_TRY_CUDA(cudaEventCreate(&e1));
     int s = MTT_OK;
-    for (int c : cands) {
-        p.threads = c;
-        if (!s) s = run_solve(b, p, st, false);   // warm
-        if (!s) s = cuda_status(cudaEventRecord(e0, st));
-        if (!s) s = run_solve(b, p, st, false);
-        if (!s) s = cuda_status(cudaEventRecord(e1, st));
-        if (!s) s = cuda_status(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        if (!s) s = cuda_status(cudaEventElapsedTime(&ms, e0, e1));
-        if (!s && ms < best_ms) { best_ms = ms; best = c; }
+    for (int sp : spans) {
+        for (int ch : chunks) {
+            if (!s) s = apply_schedule(b, sp, ch);
+            for (int c : cands) {
+                p.threads = c;
+                if (!s) s = run_solve(b, p, st, false);   // warm
+                if (!s) s = cuda_status(cudaEventRecord(e0, st));
+                if (!s) s = run_solve(b, p, st, false);
+                if (!s) s = cuda_status(cudaEventRecord(e1, st));
+                if (!s) s = cuda_status(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                if (!s) s = cuda_status(cudaEventElapsedTime(&ms, e0, e1));
+                if (!s && ms < best_ms) { best_ms = ms; best_t = c; best_span = sp; best_chunk = ch; }
+            }
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (!s) s = apply_schedule(b, best_span, best_chunk);
     if (s) return s;
-    b->tuned_threads = best;
-    if (threads) *threads = best;
+    b->tuned_threads = best_t;
+    if (threads) *threads = best_t;
     return MTT_OK;
 }
 

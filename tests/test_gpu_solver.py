@@ -253,3 +253,40 @@ def test_batches_reuse_pool_memory_and_trim(mtt, wl, cuda):
         if k == 1:
             mtt.trim_pool()
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+
+
+@pytest.mark.parametrize("hpw,chunk", [(256, 16), (128, 3), (256, 1)])
+def test_results_do_not_depend_on_the_schedule(mtt, wl, cuda, hpw, chunk):
+    """Hands per sweep warp item and terminals per CTA change only the launch
+    shape: every value is bit-identical to the default schedule."""
+    subs = wl.river_batch(n=8, seed=41, min_support=150, max_support=700, max_sizes=3)
+    p = mtt.solve_params(iters=12, alternate=True, threads=128)
+    out = []
+    for sched in ((128, 16), (hpw, chunk)):
+        b = mtt.RiverBatch(subs)
+        b.set_schedule(128, *sched)
+        assert b.schedule() == {"threads": 128, "hands_per_warp": sched[0], "term_chunk": sched[1]}
+        b.solve(p, graph=True)
+        out.append((b.results(), [b.read(i) for i in range(len(subs))]))
+        b.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    for a_, b_ in zip(out[0][1], out[1][1]):
+        for k in a_:
+            assert np.array_equal(a_[k], b_[k]), k
+
+
+def test_autotune_picks_a_schedule(mtt, wl, cuda):
+    subs = wl.river_batch(n=16, seed=42, min_support=100, max_support=400, max_sizes=2)
+    b = mtt.RiverBatch(subs)
+    p = mtt.solve_params(iters=10, alternate=True)
+    t = b.autotune(p)
+    s = b.schedule()
+    assert t in (64, 128, 256) and s["threads"] == t
+    assert s["hands_per_warp"] in (128, 256) and s["term_chunk"] in (8, 16)
+    p.threads = t
+    b.solve(p, graph=True)
+    r1 = b.results()
+    b.set_schedule(128, 128, 16)
+    b.solve(p, graph=True)
+    assert np.array_equal(r1, b.results())
+    b.close()
