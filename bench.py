@@ -31,9 +31,9 @@ METRIC = "batched river solves/s at <=0.1% pot exploitability vs plain kernel; e
 # DRAM bytes (read + write) of one CFR iteration of the sweeps and terminals
 # (k_fwd x6, k_term x6, k_bwd x12) on the default workload (4096 subgames,
 # seed 2), from a one-pass ncu capture of dram__bytes_read.sum +
-# dram__bytes_write.sum over 26 complete iterations (min 13.167, max 13.179 GB);
+# dram__bytes_write.sum over 26 complete iterations (min 13.435, max 13.498 GB);
 # the algorithmic bytes of the same iteration are 14.251 GB.
-TRAFFIC_PER_ITER = {"subgames": 4096, "seed": 2, "bytes": 13.175e9}
+TRAFFIC_PER_ITER = {"subgames": 4096, "seed": 2, "bytes": 13.484e9}
 
 
 def parse():
