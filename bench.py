@@ -21,6 +21,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -92,7 +93,7 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mtt_bench_clocks_gpu{gpu_index}_{os.getpid()}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -319,7 +320,7 @@ def other_configs(mtt, wl, stream):
         "train_s": train_s, "train_samples": int(len(X)),
         "workload": "turn spot pot 100, stack 150, bets 50/100% + all-in, 1 raise, Dirichlet(0.3) ranges (1,128 "
                     "combos), 300 alternating CFR+ iterations: full turn + river tree vs 5 depth-limit leaves valued "
-                    "by check-down (fixed-point scans) or check-down + leaf network; leaf MAE judged at 3 held-out "
+                    "by check-down (fixed-point scans) or check-down + leaf network; leaf MAE measured at 3 held-out "
                     "spots' leaves against their full solve"}
     net.close()
     return out

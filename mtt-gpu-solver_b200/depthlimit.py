@@ -3,7 +3,7 @@
 A turn subgame is built twice from the same spot:
 - full: every turn betting round that closes with chips behind deals the
   river (48 cards) and plays a river round with the same sizes.  This is the
-  fallback, and the judge of the depth-limited solve's error.
+  fallback, and the reference for the depth-limited solve's error.
 - depth-limited (river_leaves): those rounds end in a NODE_LEAF.  Its river
   values come from the leaf network, per river card, on both players' current
   reach.  The solver evaluates it inside every pass of every iteration
@@ -13,7 +13,7 @@ The network is trained on river subgames the batched solver generates, with
 the same bet sizes and raise cap as the spot's river rounds.  Their stacks
 are the chips behind / pot ratios of the spot's leaves.  The network predicts
 the residual over check-down values.  Check-down leaves, i.e. the same solve
-with no network, are the method the network is judged against.
+with no network, are the method the network is compared with.
 """
 import numpy as np
 
@@ -122,7 +122,7 @@ def errors(spot, approx, full):
 
 
 def leaf_errors_in_situ(spot, net, iters=300, residual=True):
-    """The leaf estimates judged at the spot's own leaves against the full
+    """The leaf estimates measured at the spot's own leaves against the full
     solve.  The full turn + river subgame is solved (alternating CFR+,
     `iters`).  At every river chance node that closes a turn round with chips
     behind (a depth-limit leaf of the limited tree), both players' final

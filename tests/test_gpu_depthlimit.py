@@ -1,6 +1,6 @@
 """Depth-limited turn solving: leaf nodes valued per river card inside the
 solver's iteration (check-down by the fixed-point showdown scan, plus the
-leaf network's correction), judged against the full turn + river solve.
+leaf network's correction), measured against the full turn + river solve.
 
 Tolerances (all written here):
   * leaf values with check-down alone against the host aggregation of the
@@ -101,7 +101,7 @@ def test_leaf_batch_rejects_unset_leaves_and_best_response(mtt, dl, cuda):
 
 def test_depth_limited_solve_against_the_full_solve(mtt, dl, cuda):
     """The network is trained on leaf samples from full solves of 64 seeded
-    spots (the distribution the depth-limited solve queries), then judged
+    spots (the distribution the depth-limited solve queries), then measured
     at the leaves of three held-out spots against their full solve, next to
     check-down leaves, and the depth-limited solves are compared with the
     full solve at the turn root.  The numbers are printed; the assertions

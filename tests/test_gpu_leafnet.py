@@ -77,7 +77,7 @@ def test_adam_step_and_learning(ln, cuda):
 
 
 def test_trained_net_improves_on_check_down_leaves_and_beats_solving_time(ln, mtt, cuda):
-    """Train on river values the batched solver generates, then judge on
+    """Train on river values the batched solver generates, then measure on
     held-out subgames against their full river solve.  The method without
     the network estimates a leaf by checking the river down; the network
     learns the correction for river betting on top of it (its output layer
