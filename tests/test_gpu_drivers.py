@@ -14,6 +14,16 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "mtt-gpu-solver_b200", "bin")
 
 
+@pytest.fixture(scope="module", autouse=True)
+def _drivers_built():
+    """Builds the drivers when a checkout has only the library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mtt_build", os.path.join(ROOT, "mtt-gpu-solver_b200", "build.py"))
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    b.build_drivers(quiet=True)
+
+
 def _run(args, cwd=None):
     r = subprocess.run([os.path.join(BIN, args[0])] + args[1:], capture_output=True, text=True, timeout=600, cwd=cwd)
     assert r.returncode == 0, r.stdout + r.stderr
