@@ -198,8 +198,9 @@ def other_configs(mtt, wl, stream):
     """Device-timed numbers of the other workloads (one run each, after a
     warm-up run): the single river subgame, the turn+river DCFR solve, the
     differentiable EV over 1,024 boards, the four-player ICM river, the leaf
-    network's GEMM and training step, the preflop chain and the full flop-EV
-    dump."""
+    network's GEMM and training step, the preflop chain, the full flop-EV
+    dump, the flop-subset selection, the flop subgame and the depth-limited
+    turn solve."""
     import torch
     out = {}
     # single river subgame, uniform ranges, 1,000 CFR+ iterations + FP64 exploitability
@@ -285,6 +286,15 @@ def other_configs(mtt, wl, stream):
     mtt.ev_dump(f4[:8])
     out["ev_dump_1755"] = {"ms": _event_ms(lambda: mtt.ev_dump(f4), stream),
                            "workload": "all 1,755 canonical flops, reference runout subsample (bit-exact dump)"}
+    # flop subset by NN-OMP over the regenerated dump
+    subset = importlib.import_module("mtt-gpu-solver_b200.subset")
+    cols = mtt.ev_dump(f4).reshape(1755, -1)
+    colw = mtt.canonical_flops()[:, 3].astype(np.float64)
+    subset.nnomp(cols, colw, 100)
+    out["flop_subset_nnomp"] = {"ms": _event_ms(lambda: subset.nnomp(cols, colw, 100), stream),
+                                "workload": "optimize_subset.py on the device: 100 greedy NN-OMP steps over the "
+                                            "1,755 x 1,352 dump (resident), FP64 Lawson-Hanson refits; one "
+                                            "mtt_subset_nnomp call including its weight upload and result read-back"}
     # flop subgame: flop and turn betting, 49 turn cards, river run out
     sub = wl.flop_runout(seed=9)
     b = mtt.RiverBatch([sub])

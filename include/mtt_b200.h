@@ -434,6 +434,34 @@ int mtt_pf_read_subset(const char* path, uint8_t* h_flops, float* h_weights, int
  * suited, offsuit); -1 if invalid. */
 int mtt_pf_combo_class(int32_t c1, int32_t c2);
 
+/* ------------------------------------------- flop subset (NN-OMP, FP64) */
+/* Greedy non-negative orthogonal matching pursuit over the columns of a
+ * flop-major matrix, replacing scripts/optimize_subset.py:29-50 (which
+ * produces data/mtt_subset.bin from mtt_ev_dump_1755.bin).  Column j is
+ * d_cols[j * nfeat .. + nfeat) (the dump read as [1755][1352] f32 is the
+ * reference's A^T); d_colw: ncols FP64 column weights (the orbit weights of
+ * mtt_canonical_flops).  The target is b = A colw / sum(colw).  Each of the
+ * nselect steps adds the unselected column with the largest <A_j, r> / |A_j|
+ * (the first on ties), then refits the non-negative least-squares weights of
+ * all selected columns to b (Lawson-Hanson, FP64) and sets r = b - A_sel x.
+ * Writes d_idx[nselect] (selection order) and d_w[nselect], the last fit's
+ * weights scaled to sum to ncols.  Same selections as the reference on the
+ * shipped dump, and weights within FP64 rounding of scipy's.  Inputs must be
+ * finite.  nselect <= min(ncols, MTT_SUBSET_MAX_SELECT).  Returns
+ * MTT_ERR_UNSUPPORTED if a least-squares subproblem is rank-deficient or takes
+ * more than 3 * (columns) passive-set solves (scipy.optimize.nnls raises for
+ * the latter).  Synchronises the stream. */
+#define MTT_SUBSET_MAX_SELECT 128
+int mtt_subset_nnomp(const float* d_cols, int32_t ncols, int32_t nfeat, const double* d_colw,
+                     int32_t nselect, int32_t* d_idx, double* d_w, void* stream);
+/* Write a selection as the reference does (optimize_subset.py:52-65): bin_path
+ * gets uint32 n, then per flop c1, c2, c3, 0 (u8) and the weight as f32;
+ * txt_path gets one "<card><card><card>:<weight %.4f>" line per flop (cards
+ * as "As", "Td", ...).  h_flops3: 3 cards per flop.  Either path may be NULL.
+ * Host only. */
+int mtt_subset_write(const char* bin_path, const char* txt_path, const uint8_t* h_flops3, const double* h_w,
+                     int32_t n);
+
 /* ------------------------------------------- ICM (Malmuth-Harville, FP64) */
 /* Tournament equity of n seats with chip stacks[n] and m payouts[m] (prize
  * for 1st, 2nd, ...): the probability that seat i finishes k-th is the

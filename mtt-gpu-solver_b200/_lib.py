@@ -137,6 +137,8 @@ def lib():
         "mtt_pf_dcfr": ([vp, vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_pf_read_subset": ([ctypes.c_char_p, vp, vp, i32, vp], ctypes.c_int),
         "mtt_pf_combo_class": ([i32, i32], ctypes.c_int),
+        "mtt_subset_nnomp": ([vp, i32, i32, vp, i32, vp, vp, vp], ctypes.c_int),
+        "mtt_subset_write": ([ctypes.c_char_p, ctypes.c_char_p, vp, vp, i32], ctypes.c_int),
         "mtt_icm_equity": ([vp, i32, vp, i32, vp], ctypes.c_int),
         "mtt_icm_bubble_factors": ([vp, i32, vp, i32, vp, i32, vp], ctypes.c_int),
         "mtt_mw_tree_build": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),

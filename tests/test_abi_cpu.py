@@ -162,7 +162,8 @@ def test_flop_tree_turn_chance_and_river_runout(mtt):
 
 def test_command_line_drivers_build_and_print_usage():
     """The reference's executables (Makefile: ev_dumper, preflop_gen,
-    hu_solver, multiway_solver), built over the C ABI; --help needs no GPU."""
+    hu_solver, multiway_solver) and its subset script (subset_optimizer),
+    built over the C ABI; --help needs no GPU."""
     import importlib.util
     import os
     import subprocess
@@ -171,7 +172,8 @@ def test_command_line_drivers_build_and_print_usage():
     b = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(b)
     exes = b.build_drivers(quiet=True)
-    assert sorted(os.path.basename(e) for e in exes) == ["ev_dumper", "hu_solver", "multiway_solver", "preflop_gen"]
+    assert sorted(os.path.basename(e) for e in exes) == ["ev_dumper", "hu_solver", "multiway_solver", "preflop_gen",
+                                                                  "subset_optimizer"]
     for e in exes:
         r = subprocess.run([e, "--help"], capture_output=True, text=True, timeout=60)
         assert r.returncode == 0 and r.stdout.startswith("usage: " + os.path.basename(e)), (e, r.stdout, r.stderr)

@@ -1,6 +1,9 @@
 """The command-line drivers on the GPU, against the library API on the same
 inputs: ev_dumper's file bit for bit, preflop_gen's printed table, hu_solver's
-printed values and exploitability, multiway_solver's run."""
+printed values and exploitability, multiway_solver's run; ev_dumper then
+subset_optimizer reproduce the reference's shipped subset files."""
+import hashlib
+import json
 import os
 import re
 import subprocess
@@ -80,3 +83,17 @@ def test_hu_solver_flop_subgame_and_multiway_solver_run(mtt, cuda):
     out = _run(["multiway_solver", "--iters", "20"])
     evs = [float(x) for x in re.findall(r"EV (-?[0-9.]+) bb", out)]
     assert len(evs) == 4 and all(np.isfinite(evs))
+
+
+def test_ev_dumper_then_subset_optimizer_reproduce_the_shipped_subset(tmp_path):
+    # the reference's pipeline: ev_dumper writes the dump, optimize_subset.py
+    # turns it into mtt_subset.bin and mtt_subset_weights.txt
+    meta = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
+    _run(["ev_dumper"], cwd=tmp_path)
+    dump = (tmp_path / "mtt_ev_dump_1755.bin").read_bytes()
+    assert hashlib.sha256(dump).hexdigest() == meta["ev_dump_sha256"]
+    out = _run(["subset_optimizer"], cwd=tmp_path)
+    assert "Subset generated: 100 flops saved to mtt_subset.bin" in out
+    assert hashlib.sha256((tmp_path / "mtt_subset.bin").read_bytes()).hexdigest() == meta["subset_sha256"]
+    txt = (tmp_path / "mtt_subset_weights.txt").read_bytes()
+    assert hashlib.sha256(txt).hexdigest() == meta["subset_weights_sha256"]
