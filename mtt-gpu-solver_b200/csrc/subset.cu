@@ -407,6 +407,8 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
                 fail = true;
                 break;
             }
+            // thread 0 decides: 2 = z is the solution, 0 = stepped back (solve
+            // again), 3 = z holds a NaN (non-finite input)
             if (tid == 0) {
                 bool pos = true;
                 for (int a = 0; a < np; ++a) pos &= m.z[a] > 0.0;
@@ -424,29 +426,38 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
                             if (al < alpha) { alpha = al; qa = a; }
                         }
                     }
-                    for (int a = 0; a < np; ++a) {
-                        const int i = m.plist[a];
-                        m.x[i] += alpha * (m.z[a] - m.x[i]);
-                    }
-                    m.x[m.plist[qa]] = 0.0;
-                    int keep = 0;
-                    for (int a = 0; a < np; ++a) {
-                        const int i = m.plist[a];
-                        if (m.x[i] > 0.0) {
-                            m.plist[keep++] = i;
-                        } else {
-                            m.x[i] = 0.0;
-                            m.inP[i] = 0;
+                    if (qa < 0) {
+                        m.misc[3] = 3;
+                    } else {
+                        for (int a = 0; a < np; ++a) {
+                            const int i = m.plist[a];
+                            m.x[i] += alpha * (m.z[a] - m.x[i]);
                         }
+                        m.x[m.plist[qa]] = 0.0;
+                        int keep = 0;
+                        for (int a = 0; a < np; ++a) {
+                            const int i = m.plist[a];
+                            if (m.x[i] > 0.0) {
+                                m.plist[keep++] = i;
+                            } else {
+                                m.x[i] = 0.0;
+                                m.inP[i] = 0;
+                            }
+                        }
+                        m.misc[0] = keep;
+                        m.misc[3] = keep == 0 ? 2 : 0;   // an empty passive set is its own solution
                     }
-                    m.misc[0] = keep;
-                    m.misc[3] = keep == 0 ? 2 : 0;   // an empty passive set is its own solution
                 }
             }
             __syncthreads();
-            const bool done = m.misc[3] == 2;
+            const int verdict = m.misc[3];
             __syncthreads();
-            if (done) {
+            if (verdict == 3) {
+                if (tid == 0) atomicOr(d.err, kErrRank);
+                fail = true;
+                break;
+            }
+            if (verdict == 2) {
                 if (tid == 0) m.misc[3] = 0;
                 break;
             }
