@@ -10,16 +10,17 @@
 //   per step s = 0 .. nselect - 1                            (optimize_subset.py:40-47)
 //     k_ss_corr   corr_j = <A_j, r> / |A_j| for every unselected column j,
 //                 one warp per column, and a (max, first index) per CTA
-//     k_ss_step   one CTA: the argmax t (the first maximum, as numpy's argmax);
-//                 the Gram row G[s][0..s] = <A_t, A_sel[p]> and h[s] = <A_t, b>;
-//                 the non-negative least-squares weights x of the selected
-//                 columns; the residual r = b - A_sel x
+//     k_ss_gram   the argmax t (the first maximum, as numpy's argmax) and the
+//                 Gram row G[s][0..s] = <A_t, A_sel[q]>, h[s] = <A_t, b>, one
+//                 warp per dot
+//     k_ss_nnls   one CTA: the non-negative least-squares weights x of the
+//                 selected columns, then the residual r = b - A_sel x
 //   output      x * ncols / sum(x)                           (optimize_subset.py:50)
 //
 // The weights come from Lawson and Hanson's active-set method ("Solving Least
 // Squares Problems", SIAM 1995, ch. 23), the algorithm of the reference's
 // scipy.optimize.nnls, here on the normal equations G x = h with an FP64
-// Cholesky factor of the passive block, started from the previous step's
+// L D L^T factor of the passive block, started from the previous step's
 // weights instead of from zero.  A full-column-rank NNLS problem has one
 // solution, so both choices change rounding only: about cond(A_sel)^2 * 2^-53
 // relative, 2e-12 for the 100 flops the shipped dump selects (condition
@@ -29,6 +30,10 @@
 // second-best correlation of every step on the shipped dump are at least
 // 8.4e-5 apart.  Every reduction runs in a fixed order: results are the same
 // on every run.
+//
+// The refit is a chain of short dependent steps on one SM: the factor takes
+// one barrier per passive column, and the triangular solves run on one warp
+// with each lane's rows in registers, one shuffle per row.
 #include <cfloat>
 #include <climits>
 #include <cstdint>
@@ -41,7 +46,7 @@ namespace mtt {
 namespace ss {
 
 constexpr int kCorrWarps = 8;          // columns per k_ss_corr CTA
-constexpr int kStepThreads = 512;      // k_ss_step CTA
+constexpr int kStepThreads = 512;      // k_ss_nnls CTA
 constexpr int kStepWarps = kStepThreads / 32;
 constexpr int kTargetChunks = 32;      // column chunks of the target's partial sums
 
@@ -101,6 +106,7 @@ __device__ __forceinline__ double lane_dot(const float* __restrict__ a, const do
     if (VEC) {
         const float4* a4 = reinterpret_cast<const float4*>(a);
         const double2* y2 = reinterpret_cast<const double2*>(y);
+#pragma unroll 4
         for (int q = lane; q < (n >> 2); q += 32) {
             const float4 v = __ldg(a4 + q);
             const double2 u0 = __ldg(y2 + 2 * q), u1 = __ldg(y2 + 2 * q + 1);
@@ -122,6 +128,7 @@ __device__ __forceinline__ double lane_dot_ff(const float* __restrict__ a, const
     if (VEC) {
         const float4* a4 = reinterpret_cast<const float4*>(a);
         const float4* c4 = reinterpret_cast<const float4*>(c);
+#pragma unroll 4
         for (int q = lane; q < (n >> 2); q += 32) {
             const float4 u = __ldg(a4 + q), v = __ldg(c4 + q);
             s = fma((double)u.x, (double)v.x, s);
@@ -207,28 +214,82 @@ __global__ void __launch_bounds__(kCorrWarps * 32) k_ss_corr(SsDev d) {
     }
 }
 
-// Shared memory of k_ss_step for subproblems of up to K columns.
+// The (max, first index) of the k_ss_corr partials, reduced by one CTA of
+// NT threads (every thread gets it); -1 when no finite correlation is left.
+template <int NT>
+__device__ __forceinline__ int ss_argmax_partials(const SsDev& d) {
+    __shared__ double av[NT / 32];
+    __shared__ int ai[NT / 32];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    double v = -INFINITY;
+    int i = INT_MAX;
+    for (int k = tid; k < d.ncorr; k += NT) amax_merge(v, i, d.part_v[k], d.part_i[k]);
+    warp_amax(v, i);
+    if (lane == 0) { av[w] = v; ai[w] = i; }
+    __syncthreads();
+    double bv = av[0];
+    int bi = ai[0];
+#pragma unroll
+    for (int k = 1; k < NT / 32; ++k) amax_merge(bv, bi, av[k], ai[k]);
+    return (bv > -INFINITY && bi < d.ncols) ? bi : -1;
+}
+
+// Step s, part 1 (optimize_subset.py:44-45): the selected column t and its
+// Gram row G[s][0..s] = <A_t, A_sel[q]> (q < s), <A_t, A_t>, and
+// h[s] = <A_t, b>: one warp per dot, s + 2 dots.
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_ss_gram(SsDev d, int s) {
+    if (*d.err) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int t = ss_argmax_partials<256>(d);
+    if (t < 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(d.err, kErrNoCandidate);
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        d.sel[s] = t;
+        d.taken[t] = 1;
+    }
+    const int q = blockIdx.x * 8 + w;
+    if (q > s + 1) return;
+    const float* At = d.A + (size_t)t * d.nfeat;
+    double v;
+    if (q <= s) {
+        const int c = q < s ? d.sel[q] : t;
+        v = warp_sum_d(lane_dot_ff<VEC>(At, d.A + (size_t)c * d.nfeat, d.nfeat, lane));
+    } else {
+        v = warp_sum_d(lane_dot<VEC>(At, d.b, d.nfeat, lane));
+    }
+    if (lane == 0) {
+        if (q <= s) d.G[tri(s) + q] = v;
+        else d.h[s] = v;
+    }
+}
+
+// Shared memory of k_ss_nnls for subproblems of up to K <= 128 columns.
 struct StepSmem {
-    double* G;      // tri(K) packed lower Gram matrix
-    double* L;      // tri(K) packed Cholesky factor of the passive block, list order
+    double* G;      // tri(K): packed lower Gram matrix of the selected columns
+    double* F;      // tri(K): LDL^T factor of the passive block, list order (see ss_factor)
     double* h;      // K
-    double* x;      // K
-    double* z;      // K, passive-set solution, list order
-    double* y;      // K
+    double* x;      // K: current weights
+    double* z;      // K: passive-set solution, list order
+    double* y;      // K: D^-1 L'^-1 h_P, list order
     double* dual;   // K
-    int* plist;     // K, the passive set in the order it was built
-    int* inP;       // K, 1 for a passive column
-    int* misc;      // [0] passive count, [1] flags, [2] chosen index, [3] done
-    static size_t bytes(int K) { return sizeof(double) * (2 * (size_t)tri(K) + 5 * (size_t)K) + sizeof(int) * (2 * (size_t)K + 8); }
+    double* invd;   // K: 1 / pivot
+    int* plist;     // K: the passive set in the order it was built
+    int* inP;       // K: 1 for a passive column
+    int* misc;      // [0] passive count, [1] pivot flag, [3] verdict
+    static size_t bytes(int K) { return sizeof(double) * (2 * (size_t)tri(K) + 6 * (size_t)K) + sizeof(int) * (2 * (size_t)K + 8); }
     __device__ void carve(void* base, int K) {
         double* p = reinterpret_cast<double*>(base);
         G = p; p += tri(K);
-        L = p; p += tri(K);
+        F = p; p += tri(K);
         h = p; p += K;
         x = p; p += K;
         z = p; p += K;
         y = p; p += K;
         dual = p; p += K;
+        invd = p; p += K;
         plist = reinterpret_cast<int*>(p);
         inP = plist + K;
         misc = inP + K;
@@ -237,137 +298,117 @@ struct StepSmem {
 
 __device__ __forceinline__ double gsym(const double* G, int i, int j) { return i >= j ? G[tri(i) + j] : G[tri(j) + i]; }
 
-// z_P = G_PP^-1 h_P by a Cholesky factor of the passive block (np >= 1),
-// computed from scratch: one barrier per column.  Returns false, in every
-// thread, when a pivot is not positive.
-__device__ bool ss_solve_passive(StepSmem& m, int np) {
+// The register of a warp-distributed vector (row i = lane + 32 g) that holds row k.
+__device__ __forceinline__ double pick4(double v0, double v1, double v2, double v3, int k) {
+    const int g = k >> 5;
+    return g == 0 ? v0 : (g == 1 ? v1 : (g == 2 ? v2 : v3));
+}
+
+// G_PP = L' D L'^T for the passive list P (np >= 1) by right-looking
+// elimination, one barrier per column.  F holds, on and below the diagonal,
+// the eliminated matrix: F(i, k) = L'(i, k) d_k and F(k, k) = d_k; invd[k] =
+// 1 / d_k, computed by the thread that finishes pivot k.  Returns false, in
+// every thread, when a pivot is not positive (a rank-deficient block).
+__device__ bool ss_factor(StepSmem& m, int np) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int* P = m.plist;
+    for (int i = w; i < np; i += kStepWarps)
+        for (int k = lane; k <= i; k += 32) m.F[tri(i) + k] = gsym(m.G, P[i], P[k]);
+    __syncthreads();
     if (tid == 0) {
-        const double d0 = m.G[tri(P[0]) + P[0]];
+        const double d0 = m.F[0];
         m.misc[1] = d0 > 0.0 ? 0 : 1;
-        m.L[0] = sqrt(fmax(d0, 0.0));
+        m.invd[0] = 1.0 / d0;
     }
     __syncthreads();
-    // column j below the diagonal; the warp that owns row j + 1 (warp 0) then
-    // finishes that row's diagonal
     for (int j = 0; j + 1 < np; ++j) {
-        const double* Lj = m.L + tri(j);
-        for (int a = j + 1 + w; a < np; a += kStepWarps) {
-            double* La = m.L + tri(a);
-            double s = 0.0;
-            for (int k = lane; k < j; k += 32) s = fma(La[k], Lj[k], s);
-            s = warp_sum_d(s);
-            const double laj = (gsym(m.G, P[a], P[j]) - s) / Lj[j];
-            if (lane == 0) La[j] = laj;
-            if (a == j + 1) {
-                __syncwarp();
-                double t = 0.0;
-                for (int k = lane; k <= j; k += 32) t = fma(La[k], La[k], t);
-                t = warp_sum_d(t);
-                const double dd = m.G[tri(P[a]) + P[a]] - t;
-                if (lane == 0) {
-                    if (!(dd > 0.0)) m.misc[1] = 1;
-                    La[a] = sqrt(fmax(dd, 0.0));
-                }
+        const double ivj = m.invd[j];
+        const double* Fj = m.F + j;   // column j: Fj[tri(k)] = F(k, j)
+        // row i = j + 1 + w + 16 r; warp 0 owns row j + 1 and lane 0 its diagonal
+        for (int i = j + 1 + w; i < np; i += kStepWarps) {
+            double* Fi = m.F + tri(i);
+            const double lij = Fi[j] * ivj;
+            for (int k = j + 1 + lane; k <= i; k += 32) Fi[k] = fma(-lij, Fj[tri(k)], Fi[k]);
+            if (i == j + 1 && lane == 0) {
+                const double dd = Fi[i];
+                if (!(dd > 0.0)) m.misc[1] = 1;
+                m.invd[i] = 1.0 / dd;
             }
         }
         __syncthreads();
     }
-    const bool bad = m.misc[1] != 0;
-    if (bad) return false;
-    if (w == 0) {
-        // L y = h_P, then L^T z = y, one warp
-        for (int a = 0; a < np; ++a) {
-            const double* La = m.L + tri(a);
-            double s = 0.0;
-            for (int k = lane; k < a; k += 32) s = fma(La[k], m.y[k], s);
-            s = warp_sum_d(s);
-            if (lane == 0) m.y[a] = (m.h[P[a]] - s) / La[a];
-            __syncwarp();
-        }
-        for (int a = np - 1; a >= 0; --a) {
-            double s = 0.0;
-            for (int k = a + 1 + lane; k < np; k += 32) s = fma(m.L[tri(k) + a], m.z[k], s);
-            s = warp_sum_d(s);
-            if (lane == 0) m.z[a] = (m.y[a] - s) / m.L[tri(a) + a];
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    return true;
+    return m.misc[1] == 0;
 }
 
-// One selection step (optimize_subset.py:44-47).
+// z = G_PP^-1 h_P from the factor, on one warp: L' u = h_P, y = D^-1 u,
+// L'^T z = y.  Each lane holds rows lane + 32 mm in registers; a step
+// broadcasts one finished row with a shuffle.
+__device__ __forceinline__ void ss_solve_warp(StepSmem& m, int np, int lane) {
+    const int* P = m.plist;
+    const int i0 = lane, i1 = lane + 32, i2 = lane + 64, i3 = lane + 96;
+    double u0 = i0 < np ? m.h[P[i0]] : 0.0, u1 = i1 < np ? m.h[P[i1]] : 0.0;
+    double u2 = i2 < np ? m.h[P[i2]] : 0.0, u3 = i3 < np ? m.h[P[i3]] : 0.0;
+    for (int k = 0; k < np; ++k) {
+        const double yk = __shfl_sync(0xFFFFFFFFu, pick4(u0, u1, u2, u3, k), k & 31) * m.invd[k];
+        if (lane == (k & 31)) m.y[k] = yk;
+        if (i0 > k && i0 < np) u0 = fma(-m.F[tri(i0) + k], yk, u0);
+        if (i1 > k && i1 < np) u1 = fma(-m.F[tri(i1) + k], yk, u1);
+        if (i2 > k && i2 < np) u2 = fma(-m.F[tri(i2) + k], yk, u2);
+        if (i3 > k && i3 < np) u3 = fma(-m.F[tri(i3) + k], yk, u3);
+    }
+    __syncwarp();
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;   // sum over k > i of F(k, i) z_k
+    for (int k = np - 1; k >= 0; --k) {
+        const double own = m.y[k] - m.invd[k] * pick4(a0, a1, a2, a3, k);   // z_k on its lane
+        const double zk = __shfl_sync(0xFFFFFFFFu, own, k & 31);
+        if (lane == (k & 31)) m.z[k] = zk;
+        const double* Fk = m.F + tri(k);
+        if (i0 < k) a0 = fma(Fk[i0], zk, a0);
+        if (i1 < k) a1 = fma(Fk[i1], zk, a1);
+        if (i2 < k) a2 = fma(Fk[i2], zk, a2);
+        if (i3 < k) a3 = fma(Fk[i3], zk, a3);
+    }
+    __syncwarp();
+}
+
+// Step s, part 2 (optimize_subset.py:46-47): the non-negative least-squares
+// weights of the selected columns (Lawson-Hanson on G x = h, started from the
+// previous step's weights), then the residual r = b - A_sel x.
 template <bool VEC>
-__global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
+__global__ void __launch_bounds__(kStepThreads) k_ss_nnls(SsDev d, int s) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (*d.err) return;
     StepSmem m;
     m.carve(smem_raw, d.nsel);
     const int n = s + 1;
-    // (1) the argmax over the CTA partials
-    {
-        __shared__ double av[kStepWarps];
-        __shared__ int ai[kStepWarps];
-        double v = -INFINITY;
-        int i = INT_MAX;
-        for (int k = tid; k < d.ncorr; k += kStepThreads) amax_merge(v, i, d.part_v[k], d.part_i[k]);
-        warp_amax(v, i);
-        if (lane == 0) { av[w] = v; ai[w] = i; }
-        __syncthreads();
-        if (tid == 0) {
-            double bv = av[0];
-            int bi = ai[0];
-            for (int k = 1; k < kStepWarps; ++k) amax_merge(bv, bi, av[k], ai[k]);
-            m.misc[2] = (bv > -INFINITY && bi < d.ncols) ? bi : -1;
-        }
-        __syncthreads();
+    for (int k = tid; k < tri(n); k += kStepThreads) m.G[k] = d.G[k];
+    for (int k = tid; k < n; k += kStepThreads) {
+        m.h[k] = d.h[k];
+        m.x[k] = k < s ? d.x[k] : 0.0;
     }
-    const int t = m.misc[2];
-    if (t < 0) {
-        if (tid == 0) atomicOr(d.err, kErrNoCandidate);
-        return;
-    }
-    if (tid == 0) {
-        d.sel[s] = t;
-        d.taken[t] = 1;
-    }
-    // (2) the Gram rows of the previous steps, this step's row and h[s]
-    for (int k = tid; k < tri(s); k += kStepThreads) m.G[k] = d.G[k];
-    for (int k = tid; k < s; k += kStepThreads) { m.h[k] = d.h[k]; m.x[k] = d.x[k]; }
-    const float* At = d.A + (size_t)t * d.nfeat;
-    for (int q = w; q <= n; q += kStepWarps) {
-        // q < s: an earlier column; q == s: A_t itself; q == n: the target b
-        double v;
-        if (q < n) {
-            const int c = q < s ? d.sel[q] : t;
-            v = warp_sum_d(lane_dot_ff<VEC>(At, d.A + (size_t)c * d.nfeat, d.nfeat, lane));
-        } else {
-            v = warp_sum_d(lane_dot<VEC>(At, d.b, d.nfeat, lane));
+    __syncthreads();
+    // the passive set starts as the previous weights' support
+    if (w == 0) {
+        int base = 0;
+        for (int c = 0; c < n; c += 32) {
+            const int i = c + lane;
+            const bool in = i < n && m.x[i] > 0.0;
+            if (i < n) m.inP[i] = in;
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, in);
+            if (in) m.plist[base + __popc(bal & ((1u << lane) - 1u))] = i;
+            base += __popc(bal);
         }
         if (lane == 0) {
-            if (q < n) { m.G[tri(s) + q] = v; d.G[tri(s) + q] = v; }
-            else { m.h[s] = v; d.h[s] = v; }
+            m.misc[0] = base;
+            m.misc[3] = 0;
         }
-    }
-    if (tid == 0) m.x[s] = 0.0;
-    __syncthreads();
-    // (3) Lawson-Hanson from the previous weights: the passive set is their support
-    if (tid == 0) {
-        int np = 0;
-        for (int i = 0; i < n; ++i) {
-            m.inP[i] = m.x[i] > 0.0;
-            if (m.inP[i]) m.plist[np++] = i;
-        }
-        m.misc[0] = np;
-        m.misc[3] = 0;
     }
     double hmax = 0.0;
     for (int i = 0; i < n; ++i) hmax = fmax(hmax, fabs(m.h[i]));
     const double tol = 1e-10 * hmax;   // dual tolerance, far inside the shipped dump's 2.6e-6 margin
     int solves = 0;
+    bool fail = false;
     __syncthreads();
     for (;;) {
         // dual d_i = h_i - sum_k G_ik x_k, one warp per row
@@ -378,23 +419,25 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
             if (lane == 0) m.dual[i] = m.h[i] - sacc;
         }
         __syncthreads();
-        if (tid == 0) {
-            // the unconstrained index with the largest dual above tol (the first on ties)
-            int best = -1;
+        if (w == 0) {
+            // the free index with the largest dual above tol (the first on ties) joins P
             double bv = tol;
-            for (int i = 0; i < n; ++i)
+            int best = INT_MAX;
+            for (int i = lane; i < n; i += 32)
                 if (!m.inP[i] && m.dual[i] > bv) { bv = m.dual[i]; best = i; }
-            if (best < 0) {
-                m.misc[3] = 1;
-            } else {
-                m.plist[m.misc[0]++] = best;
-                m.inP[best] = 1;
+            warp_amax(bv, best);
+            if (lane == 0) {
+                if (best == INT_MAX) {
+                    m.misc[3] = 1;
+                } else {
+                    m.plist[m.misc[0]++] = best;
+                    m.inP[best] = 1;
+                }
             }
         }
         __syncthreads();
-        if (m.misc[3]) break;
-        // inner loop: solve on the passive set, step back while a weight is not positive
-        bool fail = false;
+        if (m.misc[3] == 1) break;
+        // inner loop: solve on P, step back towards the solution while a weight is not positive
         for (;;) {
             if (++solves > 3 * n) {
                 if (tid == 0) atomicOr(d.err, kErrIters);
@@ -402,50 +445,69 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
                 break;
             }
             const int np = m.misc[0];
-            if (!ss_solve_passive(m, np)) {
+            if (!ss_factor(m, np)) {
                 if (tid == 0) atomicOr(d.err, kErrRank);
                 fail = true;
                 break;
             }
-            // thread 0 decides: 2 = z is the solution, 0 = stepped back (solve
-            // again), 3 = z holds a NaN (non-finite input)
-            if (tid == 0) {
+            if (w == 0) {
+                ss_solve_warp(m, np, lane);
+                // verdict: 2 = z is the solution, 0 = stepped back, 3 = z holds a NaN
                 bool pos = true;
-                for (int a = 0; a < np; ++a) pos &= m.z[a] > 0.0;
+                for (int a = lane; a < np; a += 32) pos &= m.z[a] > 0.0;
+                pos = __all_sync(0xFFFFFFFFu, pos);
                 if (pos) {
-                    for (int a = 0; a < np; ++a) m.x[m.plist[a]] = m.z[a];
-                    m.misc[3] = 2;
+                    for (int a = lane; a < np; a += 32) m.x[m.plist[a]] = m.z[a];
+                    if (lane == 0) m.misc[3] = 2;
                 } else {
-                    // the largest step from x towards z that keeps x >= 0
-                    double alpha = INFINITY;
-                    int qa = -1;
-                    for (int a = 0; a < np; ++a) {
-                        const int i = m.plist[a];
-                        if (m.z[a] <= 0.0) {
-                            const double al = m.x[i] / (m.x[i] - m.z[a]);
-                            if (al < alpha) { alpha = al; qa = a; }
+                    // the largest step from x towards z that keeps x >= 0 (first minimum in list order)
+                    double al = INFINITY;
+                    int qa = INT_MAX;
+                    for (int a = lane; a < np; a += 32) {
+                        const double za = m.z[a];
+                        if (za <= 0.0) {
+                            const double xa = m.x[m.plist[a]];
+                            const double c = xa / (xa - za);
+                            if (c < al) { al = c; qa = a; }
                         }
                     }
-                    if (qa < 0) {
-                        m.misc[3] = 3;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const double al2 = __shfl_xor_sync(0xFFFFFFFFu, al, o);
+                        const int qa2 = __shfl_xor_sync(0xFFFFFFFFu, qa, o);
+                        if (al2 < al || (al2 == al && qa2 < qa)) { al = al2; qa = qa2; }
+                    }
+                    if (qa == INT_MAX) {
+                        if (lane == 0) m.misc[3] = 3;
                     } else {
-                        for (int a = 0; a < np; ++a) {
+                        for (int a = lane; a < np; a += 32) {
                             const int i = m.plist[a];
-                            m.x[i] += alpha * (m.z[a] - m.x[i]);
+                            m.x[i] = fma(al, m.z[a] - m.x[i], m.x[i]);
                         }
-                        m.x[m.plist[qa]] = 0.0;
-                        int keep = 0;
-                        for (int a = 0; a < np; ++a) {
-                            const int i = m.plist[a];
-                            if (m.x[i] > 0.0) {
-                                m.plist[keep++] = i;
-                            } else {
+                        __syncwarp();
+                        if (lane == 0) m.x[m.plist[qa]] = 0.0;
+                        __syncwarp();
+                        // keep the positive weights, in order
+                        int base = 0;
+                        for (int c = 0; c < np; c += 32) {
+                            const int a = c + lane;
+                            const int i = a < np ? m.plist[a] : -1;
+                            const bool keep = i >= 0 && m.x[i] > 0.0;
+                            const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+                            __syncwarp();
+                            if (keep) {
+                                m.plist[base + __popc(bal & ((1u << lane) - 1u))] = i;
+                            } else if (i >= 0) {
                                 m.x[i] = 0.0;
                                 m.inP[i] = 0;
                             }
+                            base += __popc(bal);
+                            __syncwarp();
                         }
-                        m.misc[0] = keep;
-                        m.misc[3] = keep == 0 ? 2 : 0;   // an empty passive set is its own solution
+                        if (lane == 0) {
+                            m.misc[0] = base;
+                            m.misc[3] = base == 0 ? 2 : 0;   // an empty passive set is its own solution
+                        }
                     }
                 }
             }
@@ -465,22 +527,48 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
         __syncthreads();
         if (fail) return;
     }
-    // (4) the residual r = b - A_sel x and the weights for the next step
-    for (int i = tid; i < d.nfeat; i += kStepThreads) {
-        double v = 0.0;
-        for (int p = 0; p < n; ++p) {
-            const double xp = m.x[p];
-            if (xp != 0.0) v = fma((double)__ldg(d.A + (size_t)d.sel[p] * d.nfeat + i), xp, v);
+    // the residual r = b - A_sel x over the passive columns (the weights off
+    // the passive set are zero), and the weights for the next step; the
+    // passive columns' rows and weights are staged where inP and z were
+    const int np = m.misc[0];
+    for (int a = tid; a < np; a += kStepThreads) {
+        m.inP[a] = d.sel[m.plist[a]];
+        m.z[a] = m.x[m.plist[a]];
+    }
+    __syncthreads();
+    if (VEC) {
+        const double2* b2 = reinterpret_cast<const double2*>(d.b);
+        double2* r2 = reinterpret_cast<double2*>(d.r);
+        for (int qv = tid; qv < (d.nfeat >> 2); qv += kStepThreads) {
+            double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll 8
+            for (int a = 0; a < np; ++a) {
+                const float4 u = __ldg(reinterpret_cast<const float4*>(d.A + (size_t)m.inP[a] * d.nfeat) + qv);
+                const double xa = m.z[a];
+                v0 = fma((double)u.x, xa, v0);
+                v1 = fma((double)u.y, xa, v1);
+                v2 = fma((double)u.z, xa, v2);
+                v3 = fma((double)u.w, xa, v3);
+            }
+            const double2 bl = b2[2 * qv], bh = b2[2 * qv + 1];
+            r2[2 * qv] = make_double2(bl.x - v0, bl.y - v1);
+            r2[2 * qv + 1] = make_double2(bh.x - v2, bh.y - v3);
         }
-        d.r[i] = d.b[i] - v;
+    } else {
+        for (int i = tid; i < d.nfeat; i += kStepThreads) {
+            double v = 0.0;
+#pragma unroll 8
+            for (int a = 0; a < np; ++a) v = fma((double)__ldg(d.A + (size_t)m.inP[a] * d.nfeat + i), m.z[a], v);
+            d.r[i] = d.b[i] - v;
+        }
     }
     for (int k = tid; k < n; k += kStepThreads) d.x[k] = m.x[k];
-    // (5) after the last step: the weights normalised to sum ncols (optimize_subset.py:49-50)
-    if (s + 1 == d.nsel && tid == 0) {
+    // after the last step: the weights normalised to sum ncols (optimize_subset.py:49-50)
+    if (s + 1 == d.nsel) {
         double sum = 0.0;
-        for (int p = 0; p < n; ++p) sum += m.x[p];
+        for (int p = 0; p < n; ++p) sum += m.x[p];   // every thread, the same order
         const double f = (double)d.ncols / sum;
-        for (int p = 0; p < n; ++p) {
+        for (int p = tid; p < n; p += kStepThreads) {
             d.out_idx[p] = d.sel[p];
             d.out_w[p] = m.x[p] * f;
         }
@@ -490,7 +578,7 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_step(SsDev d, int s) {
 template <bool VEC>
 int run(SsDev& d, cudaStream_t st) {
     const size_t smem = StepSmem::bytes(d.nsel);
-    MTT_TRY_CUDA(cudaFuncSetAttribute(k_ss_step<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MTT_TRY_CUDA(cudaFuncSetAttribute(k_ss_nnls<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_ss_norms<VEC><<<ceil_div(d.ncols, 8), 256, 0, st>>>(d);
     MTT_CHECK_LAUNCH();
     k_ss_target_part<<<dim3(ceil_div(d.nfeat, 256), kTargetChunks), 256, 0, st>>>(d);
@@ -500,11 +588,14 @@ int run(SsDev& d, cudaStream_t st) {
     for (int s = 0; s < d.nsel; ++s) {
         k_ss_corr<VEC><<<d.ncorr, kCorrWarps * 32, 0, st>>>(d);
         MTT_CHECK_LAUNCH();
-        k_ss_step<VEC><<<1, kStepThreads, smem, st>>>(d, s);
+        k_ss_gram<VEC><<<ceil_div(s + 2, 8), 256, 0, st>>>(d, s);
+        MTT_CHECK_LAUNCH();
+        k_ss_nnls<VEC><<<1, kStepThreads, smem, st>>>(d, s);
         MTT_CHECK_LAUNCH();
     }
     return MTT_OK;
 }
+
 
 }  // namespace ss
 }  // namespace mtt
