@@ -27,7 +27,8 @@ def _stream(s):
 
 
 def _pkg():
-    return importlib.import_module(__name__.rsplit(".", 1)[0])
+    # the package, also when this file runs as `python -m <package>.subset`
+    return importlib.import_module(__package__)
 
 
 def nnomp(cols, colw, nselect=100, stream=None):

@@ -11,6 +11,8 @@ import hashlib
 import importlib
 import json
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -95,3 +97,16 @@ def test_subset_module_cli_reads_a_dump_file(mtt, sub, cuda, tmp_path):
     dump.astype("<f4").tofile(tmp_path / "mtt_ev_dump_1755.bin")
     assert sub.main(["--dump", str(tmp_path / "mtt_ev_dump_1755.bin"), "--out-dir", str(tmp_path)]) == 0
     assert hashlib.sha256((tmp_path / "mtt_subset.bin").read_bytes()).hexdigest() == meta["subset_sha256"]
+
+
+def test_subset_module_runs_as_a_script(cuda, tmp_path):
+    # python -m <package>.subset --regenerate: the device dump, then the selection
+    meta = json.load(open(os.path.join(GOLDEN, "golden.json")))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-m", "mtt-gpu-solver_b200.subset", "--regenerate", "--out-dir", str(tmp_path)],
+                       capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Subset generated: 100 flops saved to mtt_subset.bin" in r.stdout
+    assert hashlib.sha256((tmp_path / "mtt_subset.bin").read_bytes()).hexdigest() == meta["subset_sha256"]
+    txt = (tmp_path / "mtt_subset_weights.txt").read_bytes()
+    assert hashlib.sha256(txt).hexdigest() == meta["subset_weights_sha256"]

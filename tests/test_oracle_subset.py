@@ -134,3 +134,12 @@ def test_oracle_nnomp_greedy_and_kkt():
     assert np.abs(dual[x > 0]).max() < 1e-8 * np.abs(A[:, sel].T @ b).max()
     assert (dual[x == 0] <= 1e-8 * np.abs(A[:, sel].T @ b).max()).all()
     assert np.allclose(w, x * ncols / x.sum(), rtol=1e-14, atol=0)
+
+
+def test_subset_module_finds_its_package_when_run_as_a_script():
+    # `python -m <package>.subset` runs the file as __main__; its package
+    # lookup must still return the package (no GPU needed to check that)
+    import runpy
+    g = runpy.run_module("mtt-gpu-solver_b200.subset", run_name="__main__subset_check")
+    assert g["_pkg"]().__name__ == "mtt-gpu-solver_b200"
+    assert hasattr(g["_pkg"](), "canonical_flops")
