@@ -45,3 +45,18 @@ def test_turn_counts_match_reference_kernel(mtt, cuda, tmp_path, flop):
         assert np.array_equal(got.view(np.uint32), eq.view(np.uint32)), (flop, turn)
         # padding villain slots are written as zeros, hero padding is never written
         assert not np.any(ref[t, H:, :H])
+
+
+@pytest.mark.parametrize("iters", [1, 4])
+def test_solver_matches_reference_sweep_kernels(mtt, cuda, iters):
+    # the batched solver in the reference semantics (simultaneous updates,
+    # linear averaging) against the reference's own sweep kernels, through the
+    # fixture tests/golden/make_ref_hu_golden.py made with them on a B200
+    import test_oracle_ref_hu as fx
+    sub, want = fx.load_fixture()
+    b = mtt.RiverBatch([sub])
+    b.solve(mtt.solve_params(iters=iters, algo=0, semantics=1, alternate=False, avg_power=1.0, threads=128,
+                             exploitability=False))
+    got = b.read(0)
+    b.close()
+    fx.compare(sub, want[iters], got)
