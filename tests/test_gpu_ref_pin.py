@@ -60,3 +60,18 @@ def test_solver_matches_reference_sweep_kernels(mtt, cuda, iters):
     got = b.read(0)
     b.close()
     fx.compare(sub, want[iters], got)
+
+
+@pytest.mark.parametrize("iters", [1, 4])
+def test_multiway_solver_matches_reference_kernels(mtt, cuda, iters):
+    # the four-player solver in the reference semantics against the reference's
+    # own four-player kernels, through tests/golden/make_ref_mw_golden.py's fixture
+    import importlib
+    import test_oracle_ref_mw as fx
+    mw = importlib.import_module("mtt-gpu-solver_b200.multiway")
+    sub, want = fx.load_fixture()
+    b = mw.MultiwayBatch([sub])
+    b.solve(mtt.solve_params(iters=iters, algo=0, semantics=1, avg_power=1.0))
+    got = b.read(0)
+    b.close()
+    fx.compare(sub, want[iters], got)
