@@ -102,7 +102,7 @@ typedef struct mtt_tree_spec {
     float   raise_sizes[MTT_MAX_SIZES];
     int32_t raise_cap;
     int32_t allin;                      /* 1: all-in is always offered */
-    int32_t street;                     /* 5 or 4 */
+    int32_t street;                     /* 5, 4 or 3 */
     int32_t river_leaves;               /* street 4: rounds that close with chips behind end in
                                            MTT_NODE_LEAF instead of a river chance node */
     int32_t river_runout;               /* street 4: the river is dealt straight to showdowns
@@ -142,7 +142,7 @@ int mtt_eval7(const uint8_t* d_cards7, uint32_t* d_out, int64_t n, void* stream)
  * *d_checksum = sum over hands in colex order of score*(index+1) mod 2^64.
  * If d_key_table (65,536 uint32) is given it receives key -> score for the
  * 16-bit monotone key the scans use; *d_err gets bit 1 if two scores share a
- * key.  Replaces the survey-style full enumeration of the reference scorer. */
+ * key.  No reference kernel: it checks the scorer over every 7-card hand. */
 int mtt_eval7_enumerate(uint64_t* d_hist9, uint64_t* d_checksum, uint32_t* d_key_table,
                         int32_t* d_err, void* stream);
 

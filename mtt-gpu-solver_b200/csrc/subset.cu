@@ -278,7 +278,7 @@ struct StepSmem {
     double* invd;   // K: 1 / pivot
     int* plist;     // K: the passive set in the order it was built
     int* inP;       // K: 1 for a passive column
-    int* misc;      // [0] passive count, [1] pivot flag, [3] verdict
+    int* misc;      // [0] passive count, [1] pivot flag, [3] outcome
     static size_t bytes(int K) { return sizeof(double) * (2 * (size_t)tri(K) + 6 * (size_t)K) + sizeof(int) * (2 * (size_t)K + 8); }
     __device__ void carve(void* base, int K) {
         double* p = reinterpret_cast<double*>(base);
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_nnls(SsDev d, int s) {
             }
             if (w == 0) {
                 ss_solve_warp(m, np, lane);
-                // verdict: 2 = z is the solution, 0 = stepped back, 3 = z holds a NaN
+                // outcome: 2 = z is the solution, 0 = stepped back, 3 = z holds a NaN
                 bool pos = true;
                 for (int a = lane; a < np; a += 32) pos &= m.z[a] > 0.0;
                 pos = __all_sync(0xFFFFFFFFu, pos);
@@ -512,14 +512,14 @@ __global__ void __launch_bounds__(kStepThreads) k_ss_nnls(SsDev d, int s) {
                 }
             }
             __syncthreads();
-            const int verdict = m.misc[3];
+            const int outcome = m.misc[3];
             __syncthreads();
-            if (verdict == 3) {
+            if (outcome == 3) {
                 if (tid == 0) atomicOr(d.err, kErrRank);
                 fail = true;
                 break;
             }
-            if (verdict == 2) {
+            if (outcome == 2) {
                 if (tid == 0) m.misc[3] = 0;
                 break;
             }
