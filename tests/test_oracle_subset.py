@@ -148,3 +148,20 @@ def test_subset_module_finds_its_package_when_run_as_a_script():
     r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.split() == ["mtt-gpu-solver_b200", "True"]
+
+
+def test_c_writer_matches_python_formatting_on_any_weights(mtt, tmp_path):
+    # the drop-in writer formats like the reference script for any weight: %.4f
+    # of the exact binary value (round half to even there) and f32 rounding
+    sub = __import__("importlib").import_module("mtt-gpu-solver_b200.subset")
+    rng = np.random.default_rng(5)
+    meta = pysubset.flop_meta()
+    idx = rng.choice(1755, 200, replace=False)
+    w = np.concatenate([rng.lognormal(0.0, 2.0, 180),
+                        [0.0, 5e-5, 1.5e-4, 2.5e-4, 0.00015, 0.99995, 1755.0, 1e-12, 123.45675, 3.4e38,
+                         0.125, 0.0625, 1.00005, 2.00005, 7e-5, 9.99995, 0.5, 17.55, 1e-45, 6.1e-5]])
+    cf = np.array(meta, dtype=np.uint8)
+    b, t = str(tmp_path / "w.bin"), str(tmp_path / "w.txt")
+    sub.write(b, t, cf[idx, :3], w)
+    assert open(b, "rb").read() == pysubset.subset_bin_bytes(meta, idx, w)
+    assert open(t).read() == pysubset.subset_weights_text(meta, idx, w)
