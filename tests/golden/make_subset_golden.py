@@ -11,7 +11,9 @@ output files are byte-identical to the two shipped files, and records:
   - per step, how far the selection is from a tie (relative gap between the
     best and second-best correlation) and how far each least-squares
     subproblem is from a degenerate active set (the largest dual of a zero
-    weight, and the smallest positive weight, both relative).
+    weight, and the smallest positive weight, both relative);
+  - the coefficient of determination R^2 of the final fit against the target,
+    the figure the reference's README.md:7 publishes (0.999984).
 
 Run once where the reference is mounted:
     python tests/golden/make_subset_golden.py /path/to/MTT-GPU-Solver
@@ -37,6 +39,11 @@ def main(ref_root):
     txt = pysubset.subset_weights_text(meta, idx, w)
     assert bin_bytes == open(os.path.join(ref_root, "data", "mtt_subset.bin"), "rb").read()
     assert txt == open(os.path.join(ref_root, "data", "mtt_subset_weights.txt")).read()
+    A = dump.T.astype(np.float64)
+    colw = np.array([m[3] for m in meta], np.float64)
+    target = A @ colw / colw.sum()
+    fit = A[:, idx] @ (w * (np.sum(pysubset.nnls(A[:, idx], target)[0]) / len(meta)))
+    r2 = 1.0 - np.sum((target - fit) ** 2) / np.sum((target - target.mean()) ** 2)
     out = {
         "source": "oracle/pysubset.py on MTT-GPU-Solver data/mtt_ev_dump_1755.bin; "
                   "its outputs equal data/mtt_subset.bin and data/mtt_subset_weights.txt byte for byte",
@@ -47,6 +54,7 @@ def main(ref_root):
         "step_gap": tr["gap"],
         "step_zero_dual": tr["zero_dual"],
         "step_min_weight": tr["min_weight"],
+        "fit_r2": float(r2),
     }
     with open(os.path.join(HERE, "subset_nnomp.json"), "w") as f:
         json.dump(out, f, indent=1)

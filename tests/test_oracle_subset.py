@@ -165,3 +165,8 @@ def test_c_writer_matches_python_formatting_on_any_weights(mtt, tmp_path):
     sub.write(b, t, cf[idx, :3], w)
     assert open(b, "rb").read() == pysubset.subset_bin_bytes(meta, idx, w)
     assert open(t).read() == pysubset.subset_weights_text(meta, idx, w)
+
+
+def test_fixture_fit_reproduces_published_r2(fixture):
+    # the reference's README.md:7 publishes R^2 = 0.999984 for this selection's fit
+    assert round(fixture["fit_r2"], 6) == 0.999984
