@@ -170,3 +170,30 @@ def test_c_writer_matches_python_formatting_on_any_weights(mtt, tmp_path):
 def test_fixture_fit_reproduces_published_r2(fixture):
     # the reference's README.md:7 publishes R^2 = 0.999984 for this selection's fit
     assert round(fixture["fit_r2"], 6) == 0.999984
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_oracle_nnomp_matches_the_loop_with_scipy_nnls(seed):
+    # the same greedy loop with the reference's solver (scipy.optimize.nnls) in
+    # place of the oracle's own Lawson-Hanson: same selections, same weights
+    from scipy.optimize import nnls as scipy_nnls
+    rng = np.random.default_rng(seed)
+    ncols, nfeat, k = 200, 60, 25
+    basis = rng.standard_normal((8, nfeat))
+    dump = (rng.random((ncols, 8)) @ basis + 0.4 * rng.standard_normal((ncols, nfeat))).astype(np.float32)
+    colw = rng.integers(1, 25, ncols).astype(np.float64)
+    idx, w = pysubset.nnomp(dump, colw, k)
+    A = dump.T
+    b = (A @ colw) / colw.sum()
+    An = A / np.linalg.norm(A, axis=0)
+    sel, r = [], b.copy()
+    for _ in range(k):
+        c = An.T @ r
+        c[sel] = -np.inf
+        sel.append(int(np.argmax(c)))
+        x, _ = scipy_nnls(A[:, sel], b)
+        r = b - A[:, sel] @ x
+    assert idx.tolist() == sel
+    ws = x * (ncols / x.sum())
+    assert np.array_equal(w == 0, ws == 0)
+    assert np.abs(w - ws).max() <= 1e-9 * ws.max()
