@@ -132,53 +132,135 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_solves_per_s(subs, iters, n_sample, budget_s=20.0):
-    """The CPU restatement of the reference sweeps (oracle), all host cores,
-    on a bounded sample: n_sample subgames for a fraction of the iterations,
-    scaled to full solves (the per-iteration cost does not depend on t)."""
+def host_cpu():
+    """(CPU model, logical cores) of this host."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+def workload_config(args, world):
+    """The `config` object both arms print (identical for the same flags)."""
+    return {"workload": f"batched uneven river CFR+, {args.subgames} subgames per GPU, {args.iters} alternating "
+                        f"iterations + FP64 exploitability, continued to <= {args.target * 100:g}% pot",
+            "subgames_per_gpu": args.subgames, "iters": args.iters, "seed": args.seed,
+            "gate_pct_pot": args.target * 100,
+            "l2": "inputs larger than L2 (every subgame's arrays resident: GBs per GPU)",
+            "parallelism": f"replicas x{world} (weak scaling, no data-path collective)"}
+
+
+def _oracle_modules():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
+    import pyworkload
     pyoracle.lib()
+    return pyoracle, pyworkload
+
+
+def cpu_oracle_sample(subs, iters, n_sample, budget_s=4.0):
+    """One bounded sample of the workload on the CPU restatement of the
+    reference sweeps (oracle: dense O(H^2) FP64 showdowns), all host cores:
+    n_sample subgames at once, each through `it` alternating CFR+ iterations
+    then the oracle's FP64 best response.  `it` is sized once so the sample
+    takes about budget_s.  Returns a callable that runs one sample and gives
+    (wall seconds of the sample, full-solve-equivalent seconds, it)."""
+    pyoracle, _ = _oracle_modules()
     cores = os.cpu_count() or 1
     sample = subs[:n_sample]
-    # calibrate: one iteration of the sample, then size the run to the budget
-    t0 = time.perf_counter()
-    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
-        list(ex.map(lambda g: pyoracle.cfr_solve(g, 1, alternate=1), sample))
-    t1 = time.perf_counter() - t0
-    it = int(max(1, min(iters, budget_s / max(t1, 1e-6))))
-    t0 = time.perf_counter()
-    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
-        list(ex.map(lambda g: pyoracle.cfr_solve(g, it, alternate=1), sample))
-    el = time.perf_counter() - t0
-    per_solve = el / len(sample) * (iters / it)
-    return 1.0 / per_solve, cores, f"{len(sample)} of the subgames x {it} of {iters} alternating CFR+ " \
-        f"iterations, dense O(H^2) showdowns, {cores} threads; scaled to full solves"
+    ex = concurrent.futures.ThreadPoolExecutor(max_workers=min(cores, len(sample)))
+
+    def iters_part(it):
+        t0 = time.perf_counter()
+        outs = list(ex.map(lambda g: pyoracle.cfr_solve(g, it, alternate=1, avg_power=2.0), sample))
+        return time.perf_counter() - t0, outs
+
+    t1, _ = iters_part(1)
+    it = int(max(1, min(iters, round(budget_s / max(t1, 1e-6)))))
+
+    def one():
+        ti, outs = iters_part(it)
+        t0 = time.perf_counter()
+        list(ex.map(lambda go: pyoracle.best_response(go[0], go[1]["S0"], go[1]["S1"]), zip(sample, outs)))
+        tb = time.perf_counter() - t0
+        return ti + tb, ti * (iters / it) + tb, it
+    return one, min(cores, len(sample))
 
 
 def run_reference(args, rank, world):
+    """The CPU arm: the oracle, a restatement of the reference's kernels (the
+    reference has no CPU solve path), on the host cores.  Each step is one
+    bounded sample: n subgames (one per core) through a fixed number of
+    alternating iterations plus the FP64 best response, sized to about 4 s.
+    `ms_per_step` is the time of that sample; `value` scales it to full
+    1,000-iteration solves.  The subgames come from the oracle's own
+    restatement of the workload generator, so the product library is never
+    loaded."""
     if rank != 0:
         return
-    wl = importlib.import_module("mtt-gpu-solver_b200.workloads")
-    subs = wl.river_batch(n=args.subgames, seed=args.seed)
+    _, pyworkload = _oracle_modules()
     n_sample = args.cpu_sample or max(os.cpu_count() or 1, 8)
-    vals = []
-    cores, sample = 1, ""
-    for _ in range(args.warmup + args.steps):
-        v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, n_sample, budget_s=5.0)
-        vals.append(v)
-    v = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+    subs = pyworkload.river_batch(n=n_sample, seed=args.seed)
+    one, threads = cpu_oracle_sample(subs, args.iters, n_sample)
+    for _ in range(args.warmup):
+        one()
+    wall, equiv, it = 0.0, 0.0, 1
+    for _ in range(args.steps):
+        w, e, it = one()
+        wall += w
+        equiv += e
+    steps = max(args.steps, 1)
+    v = n_sample * steps / equiv if equiv > 0 else 0.0
+    model, ncpu = host_cpu()
+    sample = (f"{n_sample} of the {args.subgames} subgames (seed {args.seed}) per step, each through {it} of "
+              f"{args.iters} alternating CFR+ iterations (dense O(H^2) FP64 showdowns) + the FP64 best response, "
+              f"{threads} threads; scaled to {args.iters}-iteration solves (the per-iteration cost does not depend "
+              f"on t); the gate continuation of the subgames above {args.target * 100:g}% pot is not sampled")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.subgames / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic (seeded)",
-            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames, {args.iters} iterations "
-                                   f"+ FP64 exploitability, continued to <= {args.target * 100:g}% pot",
-                       "subgames_per_gpu": args.subgames, "iters": args.iters, "seed": args.seed,
-                       "parallelism": "host cores (the reference has no CPU path; the oracle restates its kernels)"},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+            "data": "synthetic (seeded)", "config": workload_config(args, world),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample,
+                             "cpu_model": model, "nproc": ncpu},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def reference_kernels_leg(mtt, wl, stream, iters):
+    """The reference's own heads-up sweep kernels (oracle/_ref/ref_hu_sweeps,
+    built from honest_multistreet_solver.cu:88-249) against this build's
+    kernels on the same river subgame: 1,024 of the board's live combos for
+    both players, uniform ranges, pot 100, stack 200, a 75% bet plus all-in and
+    one raise (the reference holds three actions per node), `iters` CFR+
+    iterations with simultaneous updates and linear averaging in the
+    reference semantics, no best response.  Both timed with CUDA events after
+    a warm-up."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyref
+    if not pyref.available():
+        return {"unavailable": "oracle/_ref/ref_hu_sweeps not built (make -C oracle ref REF=<reference checkout>)"}
+    sub = wl.river_uniform(seed=0, n_hands=1024, bet_sizes=(0.75,))
+    try:
+        ref_ms, launches = pyref.run(sub, iters, timing=True)[4:]
+    except Exception as e:   # the harness refuses inputs it cannot index safely
+        return {"unavailable": f"reference harness: {e}"}
+    b = mtt.RiverBatch([sub])
+    p = mtt.solve_params(iters=iters, algo=0, semantics=1, alternate=False, avg_power=1.0, exploitability=False)
+    out = {"workload": f"river, 1,024 live combos per player, uniform ranges, pot 100, stack 200, 75% bet + all-in, "
+                       f"1 raise, {iters} CFR+ iterations (simultaneous, linear averaging, reference semantics), "
+                       f"no best response", "reference_ms": ref_ms, "reference_launches": launches}
+    for name, graph in (("plain_ms", False), ("graph_ms", True)):
+        b.solve(p, graph=graph)
+        out[name] = _event_ms(lambda: b.solve(p, graph=graph), stream)
+    b.close()
+    out["vs_reference_kernels"] = ref_ms / out["graph_ms"]
+    out["vs_reference_kernels_plain"] = ref_ms / out["plain_ms"]
+    return out
 
 
 def _event_ms(fn, stream, reps=1):
@@ -470,17 +552,19 @@ def run_b200(args, rank, world, local):
     h2d = sum(g["nodes"].nbytes + g["combos0"].nbytes + g["combos1"].nbytes + g["range0"].nbytes +
               g["range1"].nbytes for g in subs)
 
-    # the plain single-instance kernel: the same sweeps on one subgame at a
-    # time, launched level by level with no batching and no graph
+    # the plain single-instance kernel: the same solve (same parameters, gate
+    # included) on one subgame at a time, launched level by level with no
+    # batching and no graph; inputs resident, CUDA events around the solves only
     n_plain = min(8, len(subs))
+    singles = [mtt.RiverBatch([g]) for g in subs[:n_plain]]
+    singles[0].solve(p)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for g in subs[:n_plain]:
-        b1 = mtt.RiverBatch([g])
-        b1.solve(p)
-        b1.results()
+    plain_ms = _event_ms(lambda: [b1.solve(p) for b1 in singles], stream)
+    for b1 in singles:
         b1.close()
-    plain_s = (time.perf_counter() - t0) / n_plain
+    plain_value = n_plain / (plain_ms * 1e-3)
+
+    ref_kernels = reference_kernels_leg(mtt, wl, stream, args.iters) if not args.no_other else None
 
     # evaluator throughput (all C(52,7) hands)
     mtt.eval7_enumerate()
@@ -500,13 +584,8 @@ def run_b200(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
-            "config": {"workload": f"batched uneven river CFR+, {args.subgames} subgames, {args.iters} iterations "
-                                   f"+ FP64 exploitability, continued to <= {args.target * 100:g}% pot",
-                       "subgames_per_gpu": args.subgames,
-                       "iters": args.iters, "seed": args.seed, "cta_threads": threads,
-                       "schedule": sched,
-                       "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (info["device_bytes"] / 1e9),
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args, world),
+            "launch": {"cta_threads": threads, "schedule": sched, "resident_bytes": int(info["device_bytes"])},
             "exploitability_pct_pot": {"median": float(np.median(expl) * 100), "max": float(np.max(expl) * 100),
                                        "frac_le_gate": float(np.mean(expl <= args.target)),
                                        "gate": args.target * 100},
@@ -516,9 +595,11 @@ def run_b200(args, rank, world, local):
                             "frac_le_gate": float(np.mean(fixed_expl <= args.target)),
                             "max_expl_pct_pot": float(np.max(fixed_expl) * 100)},
             "evals_per_s": evals_per_s,
-            "plain_kernel": {"value": 1.0 / plain_s, "unit": "solves/s",
-                             "sample": f"{n_plain} subgames solved one at a time, level launches, no graph"},
-            "vs_plain": value / (1.0 / plain_s),
+            "plain_kernel": {"value": plain_value, "unit": "solves/s", "ms": plain_ms,
+                             "sample": f"{n_plain} subgames solved one at a time (same parameters and gate), level "
+                                       f"launches, no graph; CUDA events around the solves, inputs resident"},
+            "vs_plain": value / plain_value,
+            "reference_kernels": ref_kernels,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_unit": "DRAM bytes per CFR iteration (ncu capture of this workload)",
@@ -535,8 +616,17 @@ def run_b200(args, rank, world, local):
             "gpu_launches": int(gpu_launches),
             "other_configs": other}
     if rank == 0 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_oracle_solves_per_s(subs, args.iters, args.cpu_sample or max(os.cpu_count() or 1, 8))
-        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}
+        _, pyworkload = _oracle_modules()
+        n_sample = args.cpu_sample or max(os.cpu_count() or 1, 8)
+        one, threads_cpu = cpu_oracle_sample(pyworkload.river_batch(n=n_sample, seed=args.seed), args.iters,
+                                             n_sample, budget_s=8.0)
+        wall, equiv, it = one()
+        model, ncpu = host_cpu()
+        line["cpu_baseline"] = {"value": n_sample / equiv, "unit": "solves/s", "cores": threads_cpu, "kind": "port",
+                                "sample": f"{n_sample} subgames x {it} of {args.iters} alternating CFR+ iterations "
+                                          f"(dense O(H^2) FP64 showdowns) + FP64 best response, {threads_cpu} "
+                                          f"threads, {wall:.1f} s; scaled to full solves",
+                                "cpu_model": model, "nproc": ncpu}
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -46,6 +46,14 @@ const char* mtt_status_string(int status);
 int mtt_last_cuda_error(void);
 /* Library version string. */
 const char* mtt_version(void);
+/* Self-check of the bounded device waits (no reference counterpart).  One
+ * CTA waits on an mbarrier that no copy targets, giving up after limit_us
+ * microseconds (1 .. 2,000,000).  arrive = 0: nothing arrives, the wait runs
+ * out and the call returns MTT_ERR_TIMEOUT, the status every kernel with a
+ * bounded wait reports when it gives up; arrive != 0: one thread arrives
+ * first and the call returns MTT_OK.  No copy is left in flight either way,
+ * so the device stays usable.  Synchronous. */
+int mtt_selftest_bounded_wait(int32_t arrive, int32_t limit_us, void* stream);
 
 /* ------------------------------------------------------------- game trees */
 #define MTT_NODE_DECISION 0
@@ -166,7 +174,9 @@ int mtt_board_showdown_counts(const uint8_t* d_board, int32_t nboard, const uint
  * any H <= 1,326 on 4- and 5-card boards and H <= 384 on 3-card boards;
  * larger sizes return MTT_ERR_UNSUPPORTED before any device work.  The first
  * call on a device looks up the scratch address with that device current;
- * make that first call before any stream capture.  Calls that overlap in
+ * make that first call before any stream capture.  The address is kept per
+ * device and context: after a cudaDeviceReset the next call on that device
+ * looks it up again in the new context.  Calls that overlap in
  * time on the same device share the scratch and race: order them on one
  * stream or serialise them. */
 #define MTT_COUNTS_NOALLOC_MAX_WORDS 262144

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmtt_b200.so")
 
 MTT_OK = 0
+MTT_ERR_INVALID, MTT_ERR_CUDA, MTT_ERR_NOMEM, MTT_ERR_TIMEOUT, MTT_ERR_IO, MTT_ERR_UNSUPPORTED = 1, 2, 3, 4, 5, 6
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "timeout", 5: "io",
           6: "unsupported"}
 
@@ -94,6 +95,7 @@ def lib():
         "mtt_status_string": ([ctypes.c_int], ctypes.c_char_p),
         "mtt_last_cuda_error": ([], ctypes.c_int),
         "mtt_version": ([], ctypes.c_char_p),
+        "mtt_selftest_bounded_wait": ([i32, i32, vp], ctypes.c_int),
         "mtt_tree_build": ([vp, vp, i32, vp, vp, vp], ctypes.c_int),
         "mtt_tree_build_board": ([vp, vp, i32, vp, i32, vp, vp, vp], ctypes.c_int),
         "mtt_tree_validate": ([vp, i32, vp], ctypes.c_int),

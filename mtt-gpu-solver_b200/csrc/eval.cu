@@ -13,6 +13,7 @@
 //  * mtt_flop_ev / mtt_ev_dump: the reference dumper (mtt_ev_dumper.cu:85-168)
 //    with the same subsampled runouts, villain stride, ½ tie weight, FMA
 //    accumulation order and host aggregation, reproduced bit-exactly.
+#include <cuda.h>   // CUcontext / CUresult types only: the driver entry points are resolved at run time
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -625,17 +626,50 @@ namespace mtt {
 constexpr int kMaxDevices = 64;
 static std::mutex g_counts_scratch_mu;
 static uint32_t* g_counts_scratch_ptr[kMaxDevices] = {};
+static unsigned long long g_counts_scratch_ctx[kMaxDevices] = {};
 
-// Address of this device's scratch, looked up once per device with that device current.
+// Unique id of the calling thread's current context (0 if none or if the
+// driver does not offer the query).  Ids are never reused within a process,
+// so a context created after a cudaDeviceReset always has a new one.  The two
+// driver functions are resolved at run time, so the library does not link the
+// driver and still loads on machines without one.
+static unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
+
+// Address of this device's scratch in the current context.  It is looked up
+// with the device current on the first call in each context (the first call
+// on the device, and again after a cudaDeviceReset replaced its context).
 static int counts_scratch(uint32_t** out) {
     int dev = 0;
     MTT_TRY_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return MTT_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_counts_scratch_mu);
-    if (!g_counts_scratch_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_counts_scratch_ptr[dev] || ctx == 0 || ctx != g_counts_scratch_ctx[dev]) {
         void* p = nullptr;
-        MTT_TRY_CUDA(cudaGetSymbolAddress(&p, g_counts_scratch));
+        MTT_TRY_CUDA(cudaGetSymbolAddress(&p, g_counts_scratch));   // makes the device's context current
         g_counts_scratch_ptr[dev] = static_cast<uint32_t*>(p);
+        g_counts_scratch_ctx[dev] = current_context_id();
     }
     *out = g_counts_scratch_ptr[dev];
     return MTT_OK;

@@ -26,13 +26,18 @@
 // H hands (c1, c2); 5 board cards; range0[H], range1[H] (f32).
 // Output: R[n_infosets*3][1216], S[n_infosets*3][1216], root cfv [2][1216] (f32).
 //
-// usage: ref_hu_sweeps in.bin out.bin
+// With a third argument `time`, the harness first runs min(iters, 3) warm-up
+// iterations, resets the state, then times the `iters` iterations with CUDA
+// events on the launching stream and prints "iters_ms <ms> launches <n>".
+//
+// usage: ref_hu_sweeps in.bin out.bin [time]
 #define main mtt_reference_stub_main
 #include "honest_multistreet_solver.cu"
 #undef main
 
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 
 static_assert(sizeof(FlatNode) == 32, "FlatNode is 32 bytes");
 
@@ -55,10 +60,11 @@ __global__ void harness_river_equity(const AliveCombo* __restrict__ combos, int 
 static bool read_exact(FILE* f, void* p, size_t n) { return std::fread(p, 1, n, f) == n; }
 
 int main(int argc, char** argv) {
-    if (argc != 3) {
-        std::fprintf(stderr, "usage: ref_hu_sweeps in.bin out.bin\n");
+    if (argc != 3 && !(argc == 4 && std::strcmp(argv[3], "time") == 0)) {
+        std::fprintf(stderr, "usage: ref_hu_sweeps in.bin out.bin [time]\n");
         return 2;
     }
+    const bool timing = argc == 4;
     FILE* f = std::fopen(argv[1], "rb");
     if (!f) return 1;
     int32_t hdr[4];
@@ -148,7 +154,9 @@ int main(int argc, char** argv) {
     for (auto& l : levels) { off.push_back((int)flat.size()); flat.insert(flat.end(), l.begin(), l.end()); }
     CUDA_CHECK(cudaMemcpy(d_lv, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice));
     const unsigned sweep_blocks = (unsigned)((P + 255) / 256);
-    for (int t = 1; t <= iters; ++t) {
+    long long launches = 0;
+    auto run = [&](int n_it) {
+    for (int t = 1; t <= n_it; ++t) {
         for (int d = 0; d <= max_depth; ++d) {
             const int nd = (int)levels[d].size();
             kernel_forward_sweep<<<dim3(sweep_blocks, nd), 256>>>(d_lv + off[d], nd, d_nodes, d_deck, d_combos, d_R,
@@ -162,7 +170,30 @@ int main(int argc, char** argv) {
             kernel_backward_sweep<<<dim3(sweep_blocks, nd), 256>>>(d_lv + off[d], nd, d_nodes, d_deck, d_combos,
                                                                     d_sigma, d_reach, d_cfv, d_R, d_S, (float)t);
         }
+        launches += 2 * (max_depth + 1) + (terms.empty() ? 0 : 1);
         CUDA_CHECK(cudaGetLastError());
+    }
+    };
+    if (!timing) {
+        run(iters);
+    } else {
+        run(std::min(iters, 3));   // warm-up (module loading, clocks), then the same start state again
+        CUDA_CHECK(cudaDeviceSynchronize());
+        CUDA_CHECK(cudaMemset(d_R, 0, sizeof(float) * NI));
+        CUDA_CHECK(cudaMemset(d_S, 0, sizeof(float) * NI));
+        CUDA_CHECK(cudaMemset(d_sigma, 0, sizeof(float) * NI));
+        CUDA_CHECK(cudaMemset(d_cfv, 0, sizeof(float) * (size_t)n_nodes * 2 * P));
+        launches = 0;
+        cudaEvent_t e0, e1;
+        CUDA_CHECK(cudaEventCreate(&e0));
+        CUDA_CHECK(cudaEventCreate(&e1));
+        CUDA_CHECK(cudaEventRecord(e0, 0));
+        run(iters);
+        CUDA_CHECK(cudaEventRecord(e1, 0));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        std::printf("iters_ms %.6f launches %lld\n", ms, launches);
     }
     CUDA_CHECK(cudaDeviceSynchronize());
     std::vector<float> R(NI), S(NI), cfv(2 * P);
