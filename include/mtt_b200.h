@@ -549,10 +549,10 @@ int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw_batch** ou
  * reference kernels (kernel_4way_forward_sweep / _evaluate_terminals /
  * _backward_cfr_plus, multiway_4way_engine.cu:41-257).  Uses iters, algo,
  * alpha/beta/gamma, semantics (MTT_SEM_REFERENCE: the reference's strict
- * rank-position order, no ties; MTT_SEM_CORRECT: equal hands split the pot),
- * avg_power; one iteration is captured as a CUDA graph when graph != 0.
- * Neither semantics removes cards between the players' hands (the reference
- * does not).  Asynchronous. */
+ * rank-position order, no ties, no card removal; MTT_SEM_CORRECT: each
+ * player's hand removes its two cards from every opponent's range and equal
+ * hands split the pot; opponents are not conditioned on one another), avg_power;
+ * one iteration is captured as a CUDA graph when graph != 0.  Asynchronous. */
 int mtt_mw_batch_solve(mtt_mw_batch* b, const mtt_solve_params* prm, int32_t graph, void* stream);
 /* Per subgame and player, the EV of that player's range (chips) under the
  * average strategies: h_out[s*4 + p].  Synchronous. */

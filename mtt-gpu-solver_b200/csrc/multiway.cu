@@ -19,12 +19,18 @@
 //     reference semantics: F = prod over active o != p of the reach of o
 //       strictly before h in the rank-position order (positions break ties),
 //       value = ((pot - c_p) F - bf[p][p] c_p (prod W_o - F)) * prod_inactive W_o;
-//     correct semantics: hands of equal rank split the pot: with L_o, E_o
-//       the reach of o below and equal to h's rank,
+//     correct semantics: the hero's hand h removes its two cards from every
+//       opponent's range (card removal) and hands of equal rank split the
+//       pot: with W_o, L_o, E_o the reach of o over the hands that share no
+//       card with h (in total, ranked below h, ranked equal to h),
 //       value = (sum over subsets T of the active opponents of
 //                prod_{T} E_o prod_{not T} L_o (pot / (1 + |T|) - c_p)
-//                - bf[p][p] c_p (prod W_o - prod (L_o + E_o))) * prod_inactive W_o.
-//   No card removal between the players' hands, as in the reference.
+//                - bf[p][p] c_p (prod W_o - prod (L_o + E_o))) * prod_inactive W_o,
+//       and fold values use the same W_o.  Opponents are not conditioned on
+//       one another (two opponents' hands may share a card), the usual
+//       approximation of multiway solvers; the exact game sums over disjoint
+//       triples of opponent hands, which no per-hand scan gives.
+//   The reference semantics remove no cards, as the reference does not.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,6 +40,7 @@
 
 #include "mtt_common.h"
 #include "mtt_device.cuh"
+#include "solver_impl.cuh"   // Entry: one hand's positions in the per-card scan
 
 namespace mtt {
 namespace mw {
@@ -215,6 +222,8 @@ struct alignas(16) MDesc {
     long long rs_base[NP];      // float offsets of R_p / S_p
     long long tab_base;         // u16 offset of [pos | gstart | gend] per hand, Hp each
     long long range_base;       // float offset of [4][Hp] root ranges
+    long long ctab_base;        // u16 offset of the card-removal lists: [rank order H | per-card lists 2 H | seg 54]
+    long long cent_base;        // u16 offset of the per-hand Entry records (16-byte aligned)
     int n_nodes, H, Hp, pad;
     int rows[NP];
     float bf[NP * NP];
@@ -498,6 +507,127 @@ __global__ void __launch_bounds__(MT) k_mw_term(MwDev a, const int2* __restrict_
     }
 }
 
+// The correct semantics' terminal, one terminal per CTA: every player's
+// reach gathered into [rank order | per-card lists in rank order] (3 H
+// positions) and scanned (exclusive, FP64); per hero hand h and opponent o,
+// the masses below, equal to and in total over o's hands that share no card
+// with h are differences of that scan (as in the heads-up terminals: the
+// per-card lists of h's two cards are subtracted, the combo h itself, counted
+// in both, added back once).
+__global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
+    extern __shared__ __align__(16) double xs[];     // [NP][3 H + 1]
+    __shared__ double wb[MT / 32];
+    __shared__ double2 ct[NP][52];                   // per player and card: scan at the list start, list mass
+    const int t = blockIdx.x, tid = threadIdx.x;
+    if (t >= n) return;
+    const int node = terms[t].x, sub = terms[t].y;
+    const MDesc d = a.desc[sub];
+    const MNode nd = a.nodes[node];
+    const int H = d.H, Hp = d.Hp, N = 3 * H, X = N + 1;
+    const uint16_t* idx = a.tabs + d.ctab_base;
+    const uint16_t* seg = idx + N;
+    const Entry* ent = reinterpret_cast<const Entry*>(a.tabs + d.cent_base);
+    const long long HS = (long long)NP * Hp;
+    const int k_local = node - (int)d.node_base;
+    const float* ro[NP];
+#pragma unroll
+    for (int o = 0; o < NP; ++o) ro[o] = a.arena + d.arena_base + (long long)nd.src[o] * HS + (long long)o * Hp;
+    for (int o = 0; o < NP; ++o)
+        for (int k = tid; k < N; k += MT) xs[o * X + k] = (double)ro[o][idx[k]];
+    __syncthreads();
+    const int C = (N + MT - 1) / MT;
+    const int s0 = min(tid * C, N), s1 = min(s0 + C, N);
+    const int lane = tid & 31, wid = tid >> 5;
+    for (int o = 0; o < NP; ++o) {
+        double* x = xs + o * X;
+        double loc = 0.0;
+        for (int k = s0; k < s1; ++k) loc += x[k];
+        double inc = loc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double v = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+            if (lane >= off) inc += v;
+        }
+        double run = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+        if (lane == 0) run = 0.0;
+        if (lane == 31) wb[wid] = inc;
+        __syncthreads();
+        double base = 0.0, total = 0.0;
+#pragma unroll
+        for (int k = 0; k < MT / 32; ++k) {
+            if (k < wid) base += wb[k];
+            total += wb[k];
+        }
+        run += base;
+        for (int k = s0; k < s1; ++k) {
+            const double v = x[k];
+            x[k] = run;
+            run += v;
+        }
+        if (tid == 0) x[N] = total;
+        __syncthreads();
+    }
+    for (int i = tid; i < NP * 52; i += MT) {
+        const int o = i / 52, c = i - 52 * o;
+        const double b0 = xs[o * X + H + seg[c]];
+        ct[o][c] = make_double2(b0, xs[o * X + H + seg[c + 1]] - b0);
+    }
+    __syncthreads();
+    const int am = nd.amask;
+    float* outb = a.arena + d.arena_base + (long long)d.n_nodes * HS + (long long)k_local * HS;
+    for (int h = tid; h < Hp; h += MT) {
+        double L[NP], E[NP], W[NP];
+        if (h < H) {
+            const Entry e = ent[h];
+#pragma unroll
+            for (int o = 0; o < NP; ++o) {
+                const double* x = xs + o * X;
+                const double2 k1 = ct[o][e.c1], k2 = ct[o][e.c2];
+                const double rh = (double)ro[o][h];
+                L[o] = x[e.lt] - (x[e.c1lt] - k1.x) - (x[e.c2lt] - k2.x);
+                E[o] = x[e.le] - (x[e.c1le] - k1.x) - (x[e.c2le] - k2.x) + rh - L[o];
+                W[o] = x[H] - k1.y - k2.y + rh;
+            }
+        }
+        for (int p = 0; p < NP; ++p) {
+            double v = 0.0;
+            if (h < H) {
+                double others = 1.0;
+                for (int o = 0; o < NP; ++o) if (o != p) others *= W[o];
+                if (nd.type == MTT_NODE_FOLD) {
+                    const int w = __ffs(am) - 1;
+                    v = (p == w ? (double)nd.pot - (double)nd.c[p] : -(double)d.bf[p * NP + w] * (double)nd.c[p]) * others;
+                } else if (!((am >> p) & 1)) {
+                    v = -(double)d.bf[p * NP + p] * (double)nd.c[p] * others;
+                } else {
+                    const double loss = -(double)d.bf[p * NP + p] * (double)nd.c[p];
+                    double inact = 1.0, PW = 1.0, LE = 1.0, Lk[NP - 1], Ek[NP - 1];
+                    int no = 0;
+                    for (int o = 0; o < NP; ++o) {
+                        if (o == p) continue;
+                        if ((am >> o) & 1) {
+                            Lk[no] = L[o]; Ek[no] = E[o];
+                            PW *= W[o];
+                            LE *= L[o] + E[o];
+                            ++no;
+                        } else {
+                            inact *= W[o];
+                        }
+                    }
+                    double share = 0.0;
+                    for (int T = 0; T < (1 << no); ++T) {
+                        double pr = 1.0;
+                        for (int i = 0; i < no; ++i) pr *= ((T >> i) & 1) ? Ek[i] : Lk[i];
+                        share += pr * ((double)nd.pot / (1 + __popc(T)) - (double)nd.c[p]);
+                    }
+                    v = (share + loss * (PW - LE)) * inact;
+                }
+            }
+            outb[(long long)p * Hp + h] = (float)v;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(MT) k_mw_root(MwDev a, int n_sub, double* out) {
     __shared__ double wb[MT / 32];
     const int s = blockIdx.x, tid = threadIdx.x;
@@ -560,6 +690,9 @@ void free_mw(mtt_mw_batch* b) {
     delete b;
 }
 
+// Dynamic shared memory of k_mw_term_cr: four scans of 3 H + 1 doubles.
+size_t term_cr_smem(const mtt_mw_batch* b) { return sizeof(double) * (size_t)NP * (3 * (size_t)b->Hmax + 1); }
+
 MwDev mw_args(const mtt_mw_batch* b, int algo, int sem) {
     MwDev a;
     a.desc = b->d_desc; a.nodes = b->d_nodes; a.tabs = b->d_tabs; a.ranges = b->d_ranges; a.arena = b->d_arena;
@@ -577,8 +710,12 @@ int launch_sweep(const mtt_mw_batch* b, const MwDev& a, int mode, cudaStream_t s
         MTT_CHECK_LAUNCH();
     }
     if (b->n_terms) {
-        const size_t smem = sizeof(double) * (size_t)NP * ((size_t)b->Hmax + 1);
-        k_mw_term<<<b->n_terms, MT, smem, st>>>(a, b->d_terms, b->n_terms);
+        if (a.semantics == MTT_SEM_CORRECT) {
+            k_mw_term_cr<<<b->n_terms, MT, term_cr_smem(b), st>>>(a, b->d_terms, b->n_terms);
+        } else {
+            const size_t smem = sizeof(double) * (size_t)NP * ((size_t)b->Hmax + 1);
+            k_mw_term<<<b->n_terms, MT, smem, st>>>(a, b->d_terms, b->n_terms);
+        }
         MTT_CHECK_LAUNCH();
     }
     for (int d = b->levels - 1; d >= 0; --d) {
@@ -603,6 +740,9 @@ int set_term_smem(const mtt_mw_batch* b) {
     const size_t smem = sizeof(double) * (size_t)NP * ((size_t)b->Hmax + 1);
     if (smem > 48 * 1024)
         MTT_TRY_CUDA(cudaFuncSetAttribute(k_mw_term, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t cr = term_cr_smem(b);
+    if (cr > 48 * 1024)
+        MTT_TRY_CUDA(cudaFuncSetAttribute(k_mw_term_cr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cr));
     return MTT_OK;
 }
 }  // namespace
@@ -695,6 +835,53 @@ extern "C" int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw
         ht.insert(ht.end(), pos.begin(), pos.end());
         ht.insert(ht.end(), gsv.begin(), gsv.end());
         ht.insert(ht.end(), gev.begin(), gev.end());
+        // card-removal lists: hands in rank order, then per card the hands
+        // holding it in rank order, the list starts, and per hand its
+        // positions in that 3 H scan (Entry; lt / le = its rank group)
+        {
+            const int H = g.H;
+            std::vector<std::vector<uint16_t>> by(52);
+            for (int i = 0; i < H; ++i) {
+                const int h = ord[i];
+                by[cards[h] & 0xFF].push_back((uint16_t)h);
+                by[cards[h] >> 8].push_back((uint16_t)h);
+            }
+            std::vector<uint16_t> seg(54, 0), cl;
+            for (int c = 0; c < 52; ++c) {
+                seg[c] = (uint16_t)cl.size();
+                cl.insert(cl.end(), by[c].begin(), by[c].end());
+            }
+            seg[52] = seg[53] = (uint16_t)cl.size();
+            while (ht.size() % 8) ht.push_back(0);
+            d.ctab_base = (long long)ht.size();
+            for (int i = 0; i < H; ++i) ht.push_back((uint16_t)ord[i]);
+            ht.insert(ht.end(), cl.begin(), cl.end());
+            ht.insert(ht.end(), seg.begin(), seg.end());
+            while (ht.size() % 8) ht.push_back(0);
+            d.cent_base = (long long)ht.size();
+            auto card_pos = [&](int c, uint32_t sv, bool upper) {
+                int k = seg[c];
+                const int end = seg[c + 1];
+                while (k < end && (sc[cl[k]] < sv || (upper && sc[cl[k]] == sv))) ++k;
+                return (uint16_t)(H + k);
+            };
+            for (int h = 0; h < H; ++h) {
+                Entry e{};
+                const int c1 = cards[h] & 0xFF, c2 = cards[h] >> 8;
+                e.lt = gsv[h];
+                e.le = gev[h];
+                e.c1lt = card_pos(c1, sc[h], false);
+                e.c1le = card_pos(c1, sc[h], true);
+                e.c2lt = card_pos(c2, sc[h], false);
+                e.c2le = card_pos(c2, sc[h], true);
+                e.c1 = (uint8_t)c1;
+                e.c2 = (uint8_t)c2;
+                e.same = (int16_t)h;
+                uint16_t w[8];
+                std::memcpy(w, &e, sizeof(e));
+                ht.insert(ht.end(), w, w + 8);
+            }
+        }
         for (int p = 0; p < NP; ++p)
             for (int h = 0; h < d.Hp; ++h) hr.push_back(h < g.H ? g.ranges[p][h] : 0.0f);
         // nodes with reach sources and depths

@@ -92,13 +92,14 @@ def diff_boards(n=1024, seed=3, n_hands=None):
     return subs, logits
 
 
-def multiway_icm(seed=4, n_hands=None, pot_bb=4.0):
+def multiway_icm(seed=4, n_hands=None, pot_bb=4.0, raise_cap=2):
     """Config 4 (four-player ICM river): eight seats with stacks drawn
     lognormal(log 20 bb, 0.5); seats 0-3 are in the hand; payouts 50/30/20;
     Malmuth-Harville bubble factors (FP64, host); a seeded river board;
     Dirichlet(0.3) ranges over the 1,326 combos with board-blocked combos
     removed (the live combos, or n_hands of them); the tree has bets {50%,
-    100%} and one pot-sized raise (677 nodes at these depths), pot_bb of dead
+    100%} and one raise size (pot), re-raised up to raise_cap times (1,585
+    nodes at seed 4's stacks; 677 with a single raise), pot_bb of dead
     money."""
     from . import multiway as mw
     rng = np.random.default_rng(seed)
@@ -110,7 +111,7 @@ def multiway_icm(seed=4, n_hands=None, pot_bb=4.0):
     if n_hands is not None:
         live = np.sort(rng.choice(live, size=n_hands, replace=False)).astype(np.uint16)
     behind = [float(np.round(s - pot_bb / 4, 3)) for s in stacks[:4]]
-    nodes, rows, _ = mw.build_tree(pot_bb, behind, [0.5, 1.0], 1.0, 1)
+    nodes, rows, _ = mw.build_tree(pot_bb, behind, [0.5, 1.0], 1.0, raise_cap)
     ranges = []
     for _ in range(4):
         w = rng.dirichlet(np.full(1326, 0.3))[live.astype(np.int64)]

@@ -759,17 +759,21 @@ int orc_softmax_ev(const orc_game* g, const double* logits0, const double* logit
 typedef struct {
     int H, n;
     int* pos; int* gs; int* ge;      /* rank position, rank-group bounds per hand */
+    uint32_t* sc;                    /* score per hand */
+    uint64_t* mask;                  /* hole-card bit mask per hand */
 } orc_mw_ctx;
 
 static void orc_mw_ranks(const orc_mw_game* g, orc_mw_ctx* c) {
     int H = g->H;
     uint32_t* sc = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(H + 1));
     int* ord = (int*)malloc(sizeof(int) * (size_t)(H + 1));
+    c->mask = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(H + 1));
     for (int h = 0; h < H; ++h) {
         uint8_t cards[7] = {g->board[0], g->board[1], g->board[2], g->board[3], g->board[4],
                             g->cards[2 * h], g->cards[2 * h + 1]};
         sc[h] = orc_score7(cards);
         ord[h] = h;
+        c->mask[h] = (1ull << g->cards[2 * h]) | (1ull << g->cards[2 * h + 1]);
     }
     /* stable insertion sort by score (ties keep index order) */
     for (int i = 1; i < H; ++i) {
@@ -787,31 +791,88 @@ static void orc_mw_ranks(const orc_mw_game* g, orc_mw_ctx* c) {
         i = j;
     }
     c->H = H;
-    free(sc); free(ord);
+    c->sc = sc;
+    free(ord);
 }
 
-/* Terminal values of all four players at node i (kernel_4way_evaluate_terminals). */
+static void orc_mw_free(orc_mw_ctx* c) { free(c->pos); free(c->gs); free(c->ge); free(c->sc); free(c->mask); }
+
+/* Terminal values of all four players at node i (kernel_4way_evaluate_terminals).
+ * Reference semantics: the reference's rank-position CDFs, no ties, no card
+ * removal.  Correct semantics: each opponent's mass is counted only over the
+ * hands that share no card with the hero's hand (the hero's own cards are
+ * removed from every opponent's range; opponents are not conditioned on one
+ * another), below (L), equal to (E) and in total (W); equal hands split the
+ * pot.  Both by direct FP64 sums. */
 static void orc_mw_terminal(const orc_mw_game* g, const orc_mw_ctx* c, int i, int sem,
                             const float* const* reach /* [4] at node i */, float* out /* [4][H] */) {
     const mtt_mw_node* nd = &g->nodes[i];
     int H = g->H;
-    double tot[4];
-    double* cdf[4];
-    for (int o = 0; o < 4; ++o) {
-        cdf[o] = (double*)calloc((size_t)H + 1, sizeof(double));
-        double* byp = (double*)calloc((size_t)H + 1, sizeof(double));
-        for (int h = 0; h < H; ++h) byp[c->pos[h]] = reach[o][h];
-        double run = 0.0;
-        for (int k = 0; k < H; ++k) { cdf[o][k] = run; run += byp[k]; }
-        cdf[o][H] = run;
-        tot[o] = run;
-        free(byp);
-    }
     int am = nd->active_mask;
+    if (sem == ORC_SEM_REFERENCE) {
+        double tot[4];
+        double* cdf[4];
+        for (int o = 0; o < 4; ++o) {
+            cdf[o] = (double*)calloc((size_t)H + 1, sizeof(double));
+            double* byp = (double*)calloc((size_t)H + 1, sizeof(double));
+            for (int h = 0; h < H; ++h) byp[c->pos[h]] = reach[o][h];
+            double run = 0.0;
+            for (int k = 0; k < H; ++k) { cdf[o][k] = run; run += byp[k]; }
+            cdf[o][H] = run;
+            tot[o] = run;
+            free(byp);
+        }
+        for (int p = 0; p < 4; ++p) {
+            double others = 1.0;
+            for (int o = 0; o < 4; ++o) if (o != p) others *= tot[o];
+            for (int h = 0; h < H; ++h) {
+                double v;
+                if (nd->type == MTT_NODE_FOLD) {
+                    int w = 0;
+                    while (!((am >> w) & 1)) ++w;
+                    v = (p == w ? (double)nd->pot_size - (double)nd->committed[p]
+                                : -(double)g->bubble[p * 4 + w] * (double)nd->committed[p]) * others;
+                } else if (!((am >> p) & 1)) {
+                    v = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p] * others;
+                } else {
+                    double gain = (double)nd->pot_size - (double)nd->committed[p];
+                    double loss = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p];
+                    double inact = 1.0, PW = 1.0, F = 1.0;
+                    for (int o = 0; o < 4; ++o) {
+                        if (o == p) continue;
+                        if ((am >> o) & 1) { PW *= tot[o]; F *= cdf[o][c->pos[h]]; } else inact *= tot[o];
+                    }
+                    v = (gain * F + loss * (PW - F)) * inact;
+                }
+                out[(size_t)p * H + h] = (float)v;
+            }
+        }
+        for (int o = 0; o < 4; ++o) free(cdf[o]);
+        return;
+    }
+    /* correct semantics: per hero hand h and opponent o, the masses of o's
+     * hands that share no card with h */
+    double* L = (double*)malloc(sizeof(double) * 4 * (size_t)H);
+    double* E = (double*)malloc(sizeof(double) * 4 * (size_t)H);
+    double* W = (double*)malloc(sizeof(double) * 4 * (size_t)H);
+    #pragma omp parallel for schedule(static)
+    for (int h = 0; h < H; ++h) {
+        for (int o = 0; o < 4; ++o) {
+            double l = 0.0, e = 0.0, w = 0.0;
+            for (int j = 0; j < H; ++j) {
+                if (c->mask[j] & c->mask[h]) continue;
+                double r = (double)reach[o][j];
+                w += r;
+                if (c->sc[j] < c->sc[h]) l += r;
+                else if (c->sc[j] == c->sc[h]) e += r;
+            }
+            L[(size_t)o * H + h] = l; E[(size_t)o * H + h] = e; W[(size_t)o * H + h] = w;
+        }
+    }
     for (int p = 0; p < 4; ++p) {
-        double others = 1.0;
-        for (int o = 0; o < 4; ++o) if (o != p) others *= tot[o];
         for (int h = 0; h < H; ++h) {
+            double others = 1.0;
+            for (int o = 0; o < 4; ++o) if (o != p) others *= W[(size_t)o * H + h];
             double v;
             if (nd->type == MTT_NODE_FOLD) {
                 int w = 0;
@@ -821,40 +882,109 @@ static void orc_mw_terminal(const orc_mw_game* g, const orc_mw_ctx* c, int i, in
             } else if (!((am >> p) & 1)) {
                 v = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p] * others;
             } else {
-                double gain = (double)nd->pot_size - (double)nd->committed[p];
                 double loss = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p];
-                double inact = 1.0, PW = 1.0;
-                int opp[3], no = 0;
+                double inact = 1.0, PW = 1.0, LE = 1.0, share = 0.0;
+                double Lk[3], Ek[3];
+                int no = 0;
                 for (int o = 0; o < 4; ++o) {
                     if (o == p) continue;
-                    if ((am >> o) & 1) { PW *= tot[o]; opp[no++] = o; } else inact *= tot[o];
+                    if ((am >> o) & 1) {
+                        Lk[no] = L[(size_t)o * H + h];
+                        Ek[no] = E[(size_t)o * H + h];
+                        PW *= W[(size_t)o * H + h];
+                        LE *= Lk[no] + Ek[no];
+                        ++no;
+                    } else {
+                        inact *= W[(size_t)o * H + h];
+                    }
                 }
-                if (sem == ORC_SEM_REFERENCE) {
-                    double F = 1.0;
-                    for (int k = 0; k < no; ++k) F *= cdf[opp[k]][c->pos[h]];
-                    v = (gain * F + loss * (PW - F)) * inact;
-                } else {
-                    double L[3], E[3], LE = 1.0, share = 0.0;
+                for (int T = 0; T < (1 << no); ++T) {
+                    double pr = 1.0;
+                    int nt = 0;
                     for (int k = 0; k < no; ++k) {
-                        L[k] = cdf[opp[k]][c->gs[h]];
-                        E[k] = cdf[opp[k]][c->ge[h]] - L[k];
-                        LE *= L[k] + E[k];
+                        if ((T >> k) & 1) { pr *= Ek[k]; ++nt; } else pr *= Lk[k];
                     }
-                    for (int T = 0; T < (1 << no); ++T) {
-                        double pr = 1.0;
-                        int nt = 0;
-                        for (int k = 0; k < no; ++k) {
-                            if ((T >> k) & 1) { pr *= E[k]; ++nt; } else pr *= L[k];
-                        }
-                        share += pr * ((double)nd->pot_size / (1 + nt) - (double)nd->committed[p]);
-                    }
-                    v = (share + loss * (PW - LE)) * inact;
+                    share += pr * ((double)nd->pot_size / (1 + nt) - (double)nd->committed[p]);
                 }
+                v = (share + loss * (PW - LE)) * inact;
             }
             out[(size_t)p * H + h] = (float)v;
         }
     }
-    for (int o = 0; o < 4; ++o) free(cdf[o]);
+    free(L); free(E); free(W);
+}
+
+/* One terminal's values under the solver's semantics (the routine the sweep
+ * below calls), for tests: out [4][H]. */
+int orc_mw_terminal_values(const orc_mw_game* g, int i, int sem, const float* const* reach, float* out) {
+    if (!g || g->H < 1 || i < 0 || i >= g->n_nodes) return MTT_ERR_INVALID;
+    orc_mw_ctx c;
+    orc_mw_ranks(g, &c);
+    orc_mw_terminal(g, &c, i, sem, reach, out);
+    orc_mw_free(&c);
+    return MTT_OK;
+}
+
+/* The exact four-player showdown of the hand (no approximation): player p's
+ * value of hand h, summed over every assignment of hands to the other three
+ * players in which all four hands are disjoint, each weighted by the product
+ * of the three reaches; fold and inactive payoffs as above, equal hands split
+ * the pot among the active players holding them.  O(H^3) per hand: small
+ * cases only (a check of how far the hero-conditioned masses above are from
+ * the exact game). */
+int orc_mw_exact_terminal(const orc_mw_game* g, int i, const float* const* reach, double* out) {
+    if (!g || g->H < 1 || i < 0 || i >= g->n_nodes) return MTT_ERR_INVALID;
+    orc_mw_ctx c;
+    orc_mw_ranks(g, &c);
+    const mtt_mw_node* nd = &g->nodes[i];
+    int H = g->H, am = nd->active_mask;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int h = 0; h < H; ++h) {
+        for (int p = 0; p < 4; ++p) {
+            int opp[3], no = 0;
+            for (int o = 0; o < 4; ++o) if (o != p) opp[no++] = o;
+            double acc = 0.0;
+            for (int j0 = 0; j0 < H; ++j0) {
+                if (c.mask[j0] & c.mask[h]) continue;
+                double r0 = (double)reach[opp[0]][j0];
+                if (r0 == 0.0) continue;
+                uint64_t m0 = c.mask[h] | c.mask[j0];
+                for (int j1 = 0; j1 < H; ++j1) {
+                    if (c.mask[j1] & m0) continue;
+                    double r1 = r0 * (double)reach[opp[1]][j1];
+                    if (r1 == 0.0) continue;
+                    uint64_t m1 = m0 | c.mask[j1];
+                    for (int j2 = 0; j2 < H; ++j2) {
+                        if (c.mask[j2] & m1) continue;
+                        double w = r1 * (double)reach[opp[2]][j2];
+                        if (w == 0.0) continue;
+                        double u;
+                        if (nd->type == MTT_NODE_FOLD) {
+                            int win = 0;
+                            while (!((am >> win) & 1)) ++win;
+                            u = p == win ? (double)nd->pot_size - (double)nd->committed[p]
+                                         : -(double)g->bubble[p * 4 + win] * (double)nd->committed[p];
+                        } else if (!((am >> p) & 1)) {
+                            u = -(double)g->bubble[p * 4 + p] * (double)nd->committed[p];
+                        } else {
+                            int js[3] = {j0, j1, j2}, beaten = 0, ties = 0;
+                            for (int k = 0; k < 3; ++k) {
+                                if (!((am >> opp[k]) & 1)) continue;
+                                if (c.sc[js[k]] > c.sc[h]) beaten = 1;
+                                else if (c.sc[js[k]] == c.sc[h]) ++ties;
+                            }
+                            u = beaten ? -(double)g->bubble[p * 4 + p] * (double)nd->committed[p]
+                                       : (double)nd->pot_size / (1 + ties) - (double)nd->committed[p];
+                        }
+                        acc += w * u;
+                    }
+                }
+            }
+            out[(size_t)p * H + h] = acc;
+        }
+    }
+    orc_mw_free(&c);
+    return MTT_OK;
 }
 
 static float orc_mw_sigma(const float* B, int H, int A, int k, int h, int avg) {
@@ -960,7 +1090,7 @@ int orc_mw_solve(const orc_mw_game* g, const orc_cfr_params* prm, float* R[4], f
             values[p] = acc;
         }
     }
-    free(reach); free(cfv); free(c.pos); free(c.gs); free(c.ge);
+    free(reach); free(cfv); orc_mw_free(&c);
     return MTT_OK;
 }
 

@@ -114,6 +114,12 @@ typedef struct orc_mw_game {
  * each player's range EV (chips) under the average strategies. */
 int orc_mw_solve(const orc_mw_game* g, const orc_cfr_params* prm, float* R[4], float* S[4], float* root_cfv,
                  double* values);
+/* The terminal values of node i under the solver's semantics: out [4][H]. */
+int orc_mw_terminal_values(const orc_mw_game* g, int i, int sem, const float* const* reach, float* out);
+/* The exact four-player showdown (all four hands disjoint) of terminal node i
+ * for the given per-player reach vectors ([4] x H): out [4][H], FP64.
+ * O(H^3) per hand: small cases only. */
+int orc_mw_exact_terminal(const orc_mw_game* g, int i, const float* const* reach, double* out);
 /* Malmuth-Harville equity by enumerating the ordered finishers of the m paid places. */
 int orc_icm_equity(const double* stacks, int n, const double* payouts, int m, double* out);
 

@@ -229,6 +229,52 @@ def mw_solve(sub, iters, algo=0, alpha=1.5, beta=0.0, gamma=2.0, semantics=0, av
     return {"R": R, "S": S, "cfv": cfv, "values": vals}
 
 
+def _mw_game(sub):
+    nodes = np.ascontiguousarray(sub["nodes"])
+    board = np.ascontiguousarray(np.asarray(sub["board"], np.uint8))
+    cards = np.ascontiguousarray(_combo_cards(sub["combos"]))
+    g = MwGame()
+    g.nodes = nodes.ctypes.data
+    g.n_nodes = len(nodes)
+    for p in range(4):
+        g.rows[p] = int(sub["rows"][p])
+    g.board = board.ctypes.data
+    g.H = len(cards)
+    g.cards = cards.ctypes.data
+    bf = np.ones(16) if sub.get("bubble") is None else np.asarray(sub["bubble"], np.float64).reshape(16)
+    for k in range(16):
+        g.bubble[k] = float(bf[k])
+    return g, (nodes, board, cards)
+
+
+def mw_terminal(sub, node, reach, semantics=0, exact=False):
+    """Values [4][H] of terminal `node` for per-player reach vectors
+    reach[4][H]: the solver's terminal (semantics 0 correct, 1 reference) or,
+    with exact=True, the exact showdown over disjoint hands (FP64, small H)."""
+    L = lib()
+    if not getattr(L, "_mwt_sig", False):
+        L.orc_mw_terminal_values.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.orc_mw_terminal_values.restype = ctypes.c_int
+        L.orc_mw_exact_terminal.argtypes = [vp, ctypes.c_int, vp, vp]
+        L.orc_mw_exact_terminal.restype = ctypes.c_int
+        L._mwt_sig = True
+    g, keep = _mw_game(sub)
+    rg = [np.ascontiguousarray(r, np.float32) for r in reach]
+    for p in range(4):
+        g.range[p] = rg[p].ctypes.data
+    pr = (ctypes.c_void_p * 4)(*[r.ctypes.data for r in rg])
+    H = g.H
+    if exact:
+        out = np.zeros((4, H), np.float64)
+        st = L.orc_mw_exact_terminal(ctypes.byref(g), int(node), pr, out.ctypes.data)
+    else:
+        out = np.zeros((4, H), np.float32)
+        st = L.orc_mw_terminal_values(ctypes.byref(g), int(node), int(semantics), pr, out.ctypes.data)
+    if st:
+        raise RuntimeError(f"multiway terminal status {st}")
+    return out
+
+
 def icm_equity(stacks, payouts):
     L = lib()
     L.orc_icm_equity.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]

@@ -66,10 +66,10 @@ def test_multiway_batch_of_uneven_subgames(mw, mtt, wl, orc, cuda):
 
 
 def test_config4_full_range_solve(mw, mtt, wl, cuda):
-    """The four-player ICM river at full size (1,081 live combos, 677 nodes),
+    """The four-player ICM river at full size (1,081 live combos, 1,585 nodes),
     200 iterations: finite values, and regret matching moved away from uniform."""
     sub = wl.multiway_icm(seed=4)
-    assert len(sub["nodes"]) == 677 and len(sub["combos"]) == 1081
+    assert len(sub["nodes"]) == 1585 and len(sub["combos"]) == 1081
     g = _solve(mw, mtt, sub, 200, graph=True)
     assert np.isfinite(g["values"]).all()
     assert all(np.isfinite(s).all() and (s >= 0).all() for s in g["S"])

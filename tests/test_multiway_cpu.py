@@ -58,3 +58,72 @@ def test_four_player_tree(mw):
     # short stacks cap the bets (no side pots): fewer nodes, still valid
     n2, r2, _ = mw.build_tree(4.0, [3, 20, 20, 20], [0.5, 1.0], 1.0, 1)
     assert 0 < len(n2) < 677
+
+
+def test_config4_tree_size(wl):
+    """The four-player configuration: bets {50%, 100%}, one pot-sized raise
+    size re-raised up to twice, at seed 4's stacks."""
+    sub = wl.multiway_icm(seed=4)
+    assert len(sub["nodes"]) == 1585 and len(sub["combos"]) == 1081
+
+
+def _no_removal_values(orc, sub, node, reach):
+    """Ties split, opponents' full masses (no card removal), for comparison."""
+    nd = sub["nodes"][node]
+    board = list(sub["board"])
+    cards = np.array([(a, b) for a in range(52) for b in range(a + 1, 52)], np.uint8)[sub["combos"].astype(np.int64)]
+    sc = orc.eval7(np.array([board + list(c) for c in cards], np.uint8)).astype(np.int64)
+    H = len(sc)
+    W = np.array([r.sum() for r in reach], np.float64)
+    L = np.array([[reach[o][sc < sc[h]].sum() for h in range(H)] for o in range(4)])
+    E = np.array([[reach[o][sc == sc[h]].sum() for h in range(H)] for o in range(4)])
+    bf = np.asarray(sub["bubble"], np.float64).reshape(4, 4)
+    am, pot, c = int(nd["active_mask"]), float(nd["pot_size"]), nd["committed"].astype(np.float64)
+    out = np.zeros((4, H))
+    for p in range(4):
+        opp = [o for o in range(4) if o != p]
+        others = np.prod(W[opp])
+        for h in range(H):
+            if nd["type"] == 1:
+                w = (am & -am).bit_length() - 1
+                out[p, h] = ((pot - c[p]) if p == w else -bf[p, w] * c[p]) * others
+            elif not (am >> p) & 1:
+                out[p, h] = -bf[p, p] * c[p] * others
+            else:
+                act = [o for o in opp if (am >> o) & 1]
+                ina = np.prod([W[o] for o in opp if not (am >> o) & 1])
+                share = 0.0
+                for T in range(1 << len(act)):
+                    pr = np.prod([E[o, h] if (T >> i) & 1 else L[o, h] for i, o in enumerate(act)])
+                    share += pr * (pot / (1 + bin(T).count("1")) - c[p])
+                LE = np.prod([L[o, h] + E[o, h] for o in act])
+                out[p, h] = (share - bf[p, p] * c[p] * (np.prod(W[act]) - LE)) * ina
+    return out
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_card_removal_moves_terminals_toward_the_exact_game(wl, orc, seed):
+    """At small sizes, the correct semantics' terminal values (each opponent's
+    mass counted over the hands that share no card with the hero) against
+    the exact four-player showdown over disjoint hands, and the same payoffs
+    with no card removal.  Removing the hero's cards roughly halves the mean
+    error; what remains is the opponents' overlaps with one another (about a
+    quarter of random opponent triples share a card), which the
+    independent-opponents model keeps."""
+    sub = wl.multiway_icm(seed=seed, n_hands=26)
+    rng = np.random.default_rng(seed)
+    reach = [rng.dirichlet(np.full(26, 0.5)).astype(np.float32) for _ in range(4)]
+    t = sub["nodes"]["type"]
+    am = sub["nodes"]["active_mask"]
+    picks = [int(np.where(t == 1)[0][0])]
+    for k in (4, 3, 2):
+        idx = np.where((t == 2) & (np.array([bin(int(x)).count("1") for x in am]) == k))[0]
+        if len(idx):
+            picks.append(int(idx[0]))
+    for node in picks:
+        exact = orc.mw_terminal(sub, node, reach, exact=True)
+        cr = orc.mw_terminal(sub, node, reach, semantics=0).astype(np.float64)
+        nr = _no_removal_values(orc, sub, node, reach)
+        e_cr, e_nr = float(np.abs(cr - exact).max()), float(np.abs(nr - exact).max())
+        m_cr, m_nr = float(np.abs(cr - exact).mean()), float(np.abs(nr - exact).mean())
+        assert e_cr < 0.85 * e_nr and m_cr < 0.65 * m_nr, (node, e_cr, e_nr, m_cr, m_nr)
