@@ -11,8 +11,11 @@
 //               accumulate) four times per stage and commits each stage back
 //               to its "empty" mbarrier, then commits the accumulator;
 //   warps 2..5  read the accumulator with tcgen05.ld (warp w owns TMEM lanes
-//               32*(w%4) .. +31 = output rows), add the bias, apply ReLU or a
-//               ReLU mask, convert and store.
+//               32*(w%4) .. +31 = output rows), 32 columns at a time, and turn
+//               each 32 x 32 block through a padded shared-memory tile (the
+//               operand ring is idle by then) so that each store instruction
+//               writes 32 consecutive columns of one row; add the bias, apply
+//               ReLU or a ReLU mask, convert and store.
 // Every mbarrier wait is bounded; a wait that gives up sets *err, the
 // producer still waits (bounded) for its own copies and the allocating warp
 // frees the TMEM before the CTA leaves.
@@ -74,15 +77,17 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+// 16 consecutive accumulator columns of this warp's 32 TMEM lanes (lane =
+// row); complete after tmem_ld_wait.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __global__ void __launch_bounds__(THREADS, 1)
 k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, void* __restrict__ C,
@@ -156,24 +161,37 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
         tc_fence_after();
         if (!ok) atomicOr(err, 1);
         const int lg = warp & 3;                     // TMEM lanes 32*lg .. 32*lg+31
-        const int row = m0 + 32 * lg + lane;
+        const int r0 = m0 + 32 * lg;
         const bool live = ok && !*(volatile int*)s_fail;
+        // this warp's 32 x 33 transpose tile in the (now idle) operand ring
+        float* P = reinterpret_cast<float*>(smem) + (warp - 2) * 32 * 33;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            uint32_t r[16];
+        for (int c = 0; c < BN; c += 32) {
+            uint32_t r[32];
             tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)c, r);
-            if (!live || row >= M) continue;
+            tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(c + 16), r + 16);
+            tmem_ld_wait();
+            if (!live || n0 + c >= N || r0 >= M) continue;   // warp-uniform
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = n0 + c + j;
-                if (col >= N) break;
-                float v = __uint_as_float(r[j]);
-                if (bias) v += bias[col];
+            for (int j = 0; j < 32; ++j) P[lane * 33 + j] = __uint_as_float(r[j]);   // (row lane, column j)
+            __syncwarp();
+            const int col = n0 + c + lane;
+            const bool cin = col < N;
+            const float b = (bias && cin) ? bias[col] : 0.0f;
+#pragma unroll 4
+            for (int i = 0; i < 32; ++i) {
+                const int row = r0 + i;
+                if (row >= M) break;
+                float v = P[i * 33 + lane];
+                if (bias) v += b;
                 if ((flags & F_RELU) && v < 0.0f) v = 0.0f;
-                if ((flags & F_MASK) && !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f)) v = 0.0f;
-                if (flags & F_OUT_BF16) reinterpret_cast<__nv_bfloat16*>(C)[(size_t)row * ldc + col] = __float2bfloat16_rn(v);
-                else reinterpret_cast<float*>(C)[(size_t)row * ldc + col] = v;
+                if (cin) {
+                    if ((flags & F_MASK) && !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f)) v = 0.0f;
+                    if (flags & F_OUT_BF16) reinterpret_cast<__nv_bfloat16*>(C)[(size_t)row * ldc + col] = __float2bfloat16_rn(v);
+                    else reinterpret_cast<float*>(C)[(size_t)row * ldc + col] = v;
+                }
             }
+            __syncwarp();
         }
     }
     tc_fence_before();

@@ -269,3 +269,173 @@ def train_on(X, T, W, meta, epochs=3, lr=1e-4, batch=512, cap=2048, net_seed=1, 
             net.train_step(Xt[idx].contiguous(), Rt[idx].contiguous(), Wt[idx].contiguous(), lr=lr, want_loss=False)
     net.check()
     return net
+
+
+def _checkdown_rows(boards, r0, r1, stream=None):
+    """Check-down values [n, 2652] (pot units, as leafnet.checkdown_values)
+    of n rows given as 5-card boards [n, 5] and full 1,326-combo reaches
+    [n, 1326] (normalised here over each board's live combos)."""
+    import ctypes
+    import torch
+    from ._lib import check, lib
+    n = len(boards)
+    out = torch.empty((n, ln.OUT), dtype=torch.float32, device="cuda")
+    if n == 0:
+        return out.cpu().numpy()
+    rs = []
+    for r in (r0, r1):
+        tot = r.sum(axis=1, keepdims=True)
+        rs.append(np.where(tot > 0, r / np.where(tot > 0, tot, 1.0), r).astype(np.float32))
+    db = torch.from_numpy(np.ascontiguousarray(boards, np.uint8)).cuda()
+    d0, d1 = torch.from_numpy(rs[0]).cuda(), torch.from_numpy(rs[1]).cuda()
+    st = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+    check("mtt_checkdown_values", lib().mtt_checkdown_values(
+        ctypes.c_void_p(db.data_ptr()), ctypes.c_void_p(d0.data_ptr()), ctypes.c_void_p(d1.data_ptr()), n,
+        ctypes.c_void_p(out.data_ptr()), st))
+    return out.cpu().numpy()
+
+
+def leaf_training_data(n_spots, seed=100, iters=300, batch_spots=128, spot_kw=None):
+    """leaf_training_set at scale: the same samples (one per river root below
+    a leaf-closing chance node of n_spots full turn + river solves), solved
+    batch_spots spots at a time and extracted with array operations, with the
+    check-down basis computed per batch.  Returns (X [n, 2706], R [n, 2652],
+    W [n, 2652]): features, residual targets (target - check-down) and
+    weights, float32."""
+    from . import NODE_CHANCE, NODE_DECISION
+    spot_kw = spot_kw or {}
+    Xs, Rs, Ws = [], [], []
+    for s0 in range(0, n_spots, batch_spots):
+        spots = [turn_spot(seed=seed + i, **spot_kw) for i in range(s0, min(n_spots, s0 + batch_spots))]
+        subs = [subgame(s, False) for s in spots]
+        b = RiverBatch(subs)
+        b.solve(solve_params(iters=iters, exploitability=False, alternate=True, avg_power=2.0), graph=True)
+        boards, r0s, r1s, xs, ts, ws = [], [], [], [], [], []
+        for i, (sp, g) in enumerate(zip(spots, subs)):
+            nodes = g["nodes"]
+            reach, cfv = b.read_vectors(i, len(nodes))
+            combos = sp["combos"].astype(np.int64)
+            H = len(combos)
+            board = [int(c) for c in sp["board"]]
+            cc = _PAIRS[combos]
+            for k in np.nonzero(nodes["type"] == NODE_CHANCE)[0]:
+                first = int(nodes[k]["children_offset"])
+                if nodes[first]["type"] != NODE_DECISION:
+                    continue
+                pot = float(nodes[k]["pot_size"])
+                spr = (sp["stack"] - (float(nodes[k]["committed"][0]) - sp["pot"] / 2)) / pot
+                ch = first + np.arange(int(nodes[k]["num_actions"]))
+                cards = nodes[ch]["turn_idx"].astype(np.int64)                        # river card per child
+                blk = (cc[None, :, 0] == cards[:, None]) | (cc[None, :, 1] == cards[:, None])   # [R, H]
+                rp = [reach[ch, p * H:(p + 1) * H].astype(np.float64) * ~blk for p in range(2)]
+                mass = [r.sum(axis=1) for r in rp]
+                ok = (mass[0] > 0) & (mass[1] > 0)
+                if not ok.any():
+                    continue
+                R = int(ok.sum())
+                x = np.zeros((R, ln.IN), np.float32)
+                t = np.zeros((R, ln.OUT), np.float32)
+                w = np.zeros((R, ln.OUT), np.float32)
+                full = [np.zeros((R, 1326)), np.zeros((R, 1326))]
+                for p in range(2):
+                    full[p][:, combos] = rp[p][ok]
+                    x[:, p * 1326 + combos] = (rp[p][ok] / mass[p][ok, None] * 1081.0).astype(np.float32)
+                    v = cfv[ch[ok], p * H:(p + 1) * H].astype(np.float64) / (pot * mass[1 - p][ok, None])
+                    t[:, p * 1326 + combos] = np.where(blk[ok], 0.0, v).astype(np.float32)
+                    w[:, p * 1326 + combos] = (~blk[ok]).astype(np.float32)
+                for c in board:
+                    x[:, 2652 + c] = 1.0
+                x[np.arange(R), 2652 + cards[ok]] = 1.0
+                x[:, 2704] = 1.0
+                x[:, 2705] = spr
+                bd = np.empty((R, 5), np.uint8)
+                bd[:, :4] = board
+                bd[:, 4] = cards[ok]
+                boards.append(bd)
+                r0s.append(full[0])
+                r1s.append(full[1])
+                xs.append(x)
+                ts.append(t)
+                ws.append(w)
+        b.close()
+        if not xs:
+            continue
+        CD = _checkdown_rows(np.concatenate(boards), np.concatenate(r0s), np.concatenate(r1s))
+        Xs.append(np.concatenate(xs))
+        Rs.append(np.concatenate(ts) - CD)
+        Ws.append(np.concatenate(ws))
+    return np.concatenate(Xs), np.concatenate(Rs), np.concatenate(Ws)
+
+
+def train_residual(X, R, W, epochs=4, lr=1e-4, batch=512, cap=2048, net_seed=1, seed=7):
+    """A residual leaf network trained on (features, residual targets,
+    weights) rows, as train_on does from leaf_training_set's output."""
+    import torch
+    dev = torch.device("cuda")
+    Xt, Rt, Wt = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (X, R, W))
+    net = ln.LeafNet(batch_cap=cap, seed=net_seed, zero_output=True)
+    rng = np.random.default_rng(seed)
+    n = len(X)
+    for _ in range(epochs):
+        perm = torch.from_numpy(rng.permutation(n)).to(dev)
+        for k in range(0, n - batch + 1, batch):
+            idx = perm[k:k + batch]
+            net.train_step(Xt[idx].contiguous(), Rt[idx].contiguous(), Wt[idx].contiguous(), lr=lr, want_loss=False)
+    net.check()
+    return net
+
+
+def evaluate(net, seeds, iters=300):
+    """The depth-limited solve against the full turn + river solve on held-out
+    spots: per spot, the root value error (pot units, errors()) and the solve
+    time (one solve call, as solve() runs it) of network leaves, check-down
+    leaves and the full tree, and the leaf MAE at the spot's leaves
+    (leaf_errors_in_situ).  Returns a dict of per-spot lists and means."""
+    import time
+    import torch
+    out = {"root_error": {"net": [], "checkdown": []}, "leaf_mae": {"net": [], "checkdown": []},
+           "solve_s": {"full": [], "net": [], "checkdown": []}}
+    for sd in seeds:
+        spot = turn_spot(seed=sd)
+        res = {}
+        for name, kw in (("full", {"limited": False}), ("net", {"limited": True, "net": net}),
+                         ("checkdown", {"limited": True, "net": None})):
+            solve(spot, iters=10, **kw)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res[name] = solve(spot, iters=iters, **kw)
+            torch.cuda.synchronize()
+            out["solve_s"][name].append(time.perf_counter() - t0)
+        for name in ("net", "checkdown"):
+            out["root_error"][name].append(errors(spot, res[name], res["full"])["value"])
+        le = leaf_errors_in_situ(spot, net, iters=iters)
+        for name in ("net", "checkdown"):
+            out["leaf_mae"][name].append(le[name])
+    out["mean"] = {k: {n: float(np.mean(v)) for n, v in d.items()} for k, d in out.items() if k != "mean"}
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    import time
+    import torch
+    ap = argparse.ArgumentParser(description="train the leaf network on solver-generated leaf samples and measure "
+                                             "depth-limited turn solving against the full solve")
+    ap.add_argument("--spots", type=int, default=1024, help="training spots (about 200 samples each)")
+    ap.add_argument("--held-out", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--iters", type=int, default=300)
+    a = ap.parse_args()
+    t0 = time.perf_counter()
+    X, R, W = leaf_training_data(a.spots, seed=100, iters=a.iters)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    net = train_residual(X, R, W, epochs=a.epochs)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ev = evaluate(net, seeds=list(range(a.held_out)), iters=a.iters)
+    print(json.dumps({"train_samples": int(len(X)), "train_spots": a.spots, "data_s": t_data, "train_s": t_train,
+                      "epochs": a.epochs, "held_out_spots": a.held_out, **ev}))
+    net.close()

@@ -215,3 +215,35 @@ def checkdown_values_fp64(meta, batch=4096):
             out[b0 + k, 1326 + c] = (ev1 / 100.0).astype(np.float32)
         rb.close()
     return out
+
+
+def gemm_timing(M=4096, N=1024, K=2752, reps=20, seed=0):
+    """Device time of the leaf network's tcgen05 GEMM on one shape
+    (C[M x N] fp32 = A[M x K] B[N x K]^T, bf16 operands): (ms per call,
+    TFLOP/s), CUDA events on the current stream after one warm-up call."""
+    import torch
+    from . import gemm_bf16
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C = torch.empty(M, N, device="cuda")
+    gemm_bf16(A, B, out=C)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        gemm_bf16(A, B, out=C)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return ms, 2.0 * M * N * K / (ms * 1e-3) / 1e12
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="time the leaf network's GEMM on one shape")
+    ap.add_argument("--shape", type=int, nargs=3, default=[4096, 1024, 2752], metavar=("M", "N", "K"))
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    ms, tf = gemm_timing(*a.shape, reps=a.reps)
+    print(f"gemm {a.shape[0]}x{a.shape[1]}x{a.shape[2]}: {ms:.4f} ms, {tf:.1f} TFLOP/s")
