@@ -331,17 +331,17 @@ def other_configs(mtt, wl, stream):
     t = _event_ms(lambda: mb.solve(p4, graph=True), stream)
     out["multiway_icm"] = {"ms": t, "nodes": int(len(sub["nodes"])), "values": mb.values()[0].tolist(),
                            "workload": "4 players, 1,081 combos, Dirichlet(0.3) ranges, Malmuth-Harville bubble "
-                                       "factors (50/30/20 over 8 seats), 200 CFR+ iterations"}
+                                       "factors (50/30/20 over 8 seats), bets 50/100% + a pot-sized raise re-raised "
+                                       "up to twice, 200 CFR+ iterations, card removal against the hero's hand and "
+                                       "split ties (correct semantics)"}
     mb.close()
     # leaf network: one GEMM of the first layer and one training step of 4,096 samples
     ln = importlib.import_module("mtt-gpu-solver_b200.leafnet")
-    A = torch.randn(4096, 2752, device="cuda").to(torch.bfloat16)
-    B = torch.randn(1024, 2752, device="cuda").to(torch.bfloat16)
-    C = torch.empty(4096, 1024, device="cuda")
-    mtt.gemm_bf16(A, B, out=C)
-    t = _event_ms(lambda: mtt.gemm_bf16(A, B, out=C), stream, reps=20)
-    flops = 2.0 * 4096 * 1024 * 2752
-    out["leaf_gemm"] = {"ms": t, "tflops": flops / (t * 1e-3) / 1e12, "shape": [4096, 1024, 2752]}
+    gt = ln.gemm_timing(4096, 1024, 2752, reps=20)
+    out["leaf_gemm"] = {"ms": gt["graph_ms"], "tflops": gt["graph_tflops"], "shape": [4096, 1024, 2752],
+                        "per_call_ms": gt["call_ms"], "per_call_tflops": gt["call_tflops"],
+                        "timing": "20 launches captured in one CUDA graph and replayed (ms per launch); per_call: "
+                                  "20 Python calls, host work between launches included"}
     net = ln.LeafNet(batch_cap=4096, seed=0)
     X = torch.randn(4096, 2706, device="cuda") * 0.5
     T = torch.randn(4096, 2652, device="cuda") * 0.3

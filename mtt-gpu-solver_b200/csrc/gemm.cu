@@ -235,6 +235,23 @@ static int make_map(CUtensorMap* map, const void* base, int rows, int cols, int 
     return r == CUDA_SUCCESS ? MTT_OK : MTT_ERR_INVALID;
 }
 
+// The kernel's shared-memory opt-in, set once per device (a per-call
+// cudaFuncSetAttribute costs host time on every launch).
+static std::mutex g_attr_mu;
+static bool g_attr_done[64] = {};
+
+static int smem_attr_once() {
+    int dev = 0;
+    MTT_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return MTT_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (!g_attr_done[dev]) {
+        MTT_TRY_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        g_attr_done[dev] = true;
+    }
+    return MTT_OK;
+}
+
 static int launch(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
                   const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st) {
     if (M <= 0 || N <= 0 || K <= 0) return M == 0 || N == 0 ? MTT_OK : MTT_ERR_INVALID;
@@ -244,7 +261,7 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     CUtensorMap ta, tb;
     MTT_TRY(make_map(&ta, A, M, K, lda, BM));
     MTT_TRY(make_map(&tb, B, N, K, ldb, BN));
-    MTT_TRY_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    MTT_TRY(smem_attr_once());
     const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
     k_gemm_bf16<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, C, M, N, K, ldc, bias,
                                                     reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err);

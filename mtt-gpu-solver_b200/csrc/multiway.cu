@@ -40,7 +40,6 @@
 
 #include "mtt_common.h"
 #include "mtt_device.cuh"
-#include "solver_impl.cuh"   // Entry: one hand's positions in the per-card scan
 
 namespace mtt {
 namespace mw {
@@ -207,6 +206,19 @@ static int validate(const mtt_mw_node* nodes, int n, const int rows[NP]) {
 }
 
 // =================================================================== device layout
+// One hand's positions in the card-removal scan [rank order (H) | per-card
+// lists (2 H)], 16 bytes: lt / le, the first hand ranked >= / > it in rank
+// order (its rank group); c1lt / c1le (c2lt / c2le), the same inside the list
+// of hands holding its first (second) card, as absolute scan positions.
+struct alignas(16) MwEntry {
+    uint16_t lt, le;
+    uint16_t c1lt, c1le;
+    uint16_t c2lt, c2le;
+    uint8_t c1, c2;
+    uint16_t pad;
+};
+static_assert(sizeof(MwEntry) == 16, "MwEntry is 16 bytes");
+
 struct alignas(16) MNode {      // 64 B
     uint8_t type, player, na, amask;
     int32_t first, row, pad0;
@@ -223,7 +235,7 @@ struct alignas(16) MDesc {
     long long tab_base;         // u16 offset of [pos | gstart | gend] per hand, Hp each
     long long range_base;       // float offset of [4][Hp] root ranges
     long long ctab_base;        // u16 offset of the card-removal lists: [rank order H | per-card lists 2 H | seg 54]
-    long long cent_base;        // u16 offset of the per-hand Entry records (16-byte aligned)
+    long long cent_base;        // u16 offset of the per-hand MwEntry records (16-byte aligned)
     int n_nodes, H, Hp, pad;
     int rows[NP];
     float bf[NP * NP];
@@ -526,7 +538,7 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     const int H = d.H, Hp = d.Hp, N = 3 * H, X = N + 1;
     const uint16_t* idx = a.tabs + d.ctab_base;
     const uint16_t* seg = idx + N;
-    const Entry* ent = reinterpret_cast<const Entry*>(a.tabs + d.cent_base);
+    const MwEntry* ent = reinterpret_cast<const MwEntry*>(a.tabs + d.cent_base);
     const long long HS = (long long)NP * Hp;
     const int k_local = node - (int)d.node_base;
     const float* ro[NP];
@@ -578,7 +590,7 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     for (int h = tid; h < Hp; h += MT) {
         double L[NP], E[NP], W[NP];
         if (h < H) {
-            const Entry e = ent[h];
+            const MwEntry e = ent[h];
 #pragma unroll
             for (int o = 0; o < NP; ++o) {
                 const double* x = xs + o * X;
@@ -837,7 +849,7 @@ extern "C" int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw
         ht.insert(ht.end(), gev.begin(), gev.end());
         // card-removal lists: hands in rank order, then per card the hands
         // holding it in rank order, the list starts, and per hand its
-        // positions in that 3 H scan (Entry; lt / le = its rank group)
+        // positions in that 3 H scan (MwEntry; lt / le = its rank group)
         {
             const int H = g.H;
             std::vector<std::vector<uint16_t>> by(52);
@@ -866,7 +878,7 @@ extern "C" int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw
                 return (uint16_t)(H + k);
             };
             for (int h = 0; h < H; ++h) {
-                Entry e{};
+                MwEntry e{};
                 const int c1 = cards[h] & 0xFF, c2 = cards[h] >> 8;
                 e.lt = gsv[h];
                 e.le = gev[h];
@@ -876,7 +888,6 @@ extern "C" int mtt_mw_batch_create(const mtt_mw_subgame* subs, int32_t n, mtt_mw
                 e.c2le = card_pos(c2, sc[h], true);
                 e.c1 = (uint8_t)c1;
                 e.c2 = (uint8_t)c2;
-                e.same = (int16_t)h;
                 uint16_t w[8];
                 std::memcpy(w, &e, sizeof(e));
                 ht.insert(ht.end(), w, w + 8);

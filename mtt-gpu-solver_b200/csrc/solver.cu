@@ -257,11 +257,13 @@ __device__ void cta_terminal(const TermInfo& ti, const TabView& tv, int q, const
         if (h < Hq) {
             const Entry et = ent[h];
             if (et.lt != 0xFFFFu) {
-                const TA b1 = Xs[Ho + seg[et.c1]], b2 = Xs[Ho + seg[et.c2]];
+                const int s1c = Ho + seg[et.c1], s2c = Ho + seg[et.c2];
+                const TA b1 = Xs[s1c], b2 = Xs[s2c];
                 const TA C1 = Xs[Ho + seg[et.c1 + 1]] - b1, C2 = Xs[Ho + seg[et.c2 + 1]] - b2;
+ 
                 const TA ps = et.same >= 0 ? Rs(et.same) : TA(0);
-                const TA W = Xs[et.lt] - (Xs[et.c1lt] - b1) - (Xs[et.c2lt] - b2);
-                const TA LE = Xs[et.le] - (Xs[et.c1le] - b1) - (Xs[et.c2le] - b2);
+                const TA W = Xs[et.lt] - (Xs[s1c + et.ltc1] - b1) - (Xs[s2c + et.ltc2] - b2);
+                const TA LE = Xs[et.le] - (Xs[s1c + et.lec1] - b1) - (Xs[s2c + et.lec2] - b2);
                 const TA Ti = LE - W + ps;
                 if (!semantics) {
                     const TA L = Tt - C1 - C2 - LE;
@@ -320,26 +322,11 @@ __device__ __forceinline__ int fx_round(float v, const FxScale& s) {
     return __float2int_rn(__fmul_rn(v, s.f));   // a power-of-two product is exact
 }
 
-// The staged opponent reach of one terminal (n4 float4 groups, 16-byte
-// aligned), rounded to fixed point in place: afterwards the same words hold
-// int32 values.  Done once per terminal unit, so the scan gathers integers
-// and every one of its 3 H positions skips the rounding.
-template <int NT>
-__device__ __forceinline__ void fx_round_in_place(float* ro, int n4, const FxScale& fs, int tid) {
-    float4* p = reinterpret_cast<float4*>(ro);
-    int4* d = reinterpret_cast<int4*>(ro);
-    for (int j = tid; j < n4; j += NT) {
-        const float4 v = p[j];
-        d[j] = make_int4(fx_round(v.x, fs), fx_round(v.y, fs), fx_round(v.z, fs), fx_round(v.w, fs));
-    }
-}
-
 // Steps (2)-(3) for chunks of C positions.  idx: the opponent's hand index of
-// each scan position; xo: the opponent's fixed-point reach; X: N + 1 ints.
-// Returns the total.
+// each scan position; X: N + 1 ints.  Returns the total.
 template <int NT, int C>
-__device__ __forceinline__ int fx_scan(const uint16_t* __restrict__ idx, const int* __restrict__ xo, int N,
-                                       int* X, int* wi, int tid) {
+__device__ __forceinline__ int fx_scan(const uint16_t* __restrict__ idx, const float* __restrict__ ro, int N,
+                                       const FxScale& fs, int* X, int* wi, int tid) {
     const int lane = tid & 31, wid = tid >> 5;
     const int s0 = min(tid * C, N);
     int xv[C];
@@ -347,13 +334,13 @@ __device__ __forceinline__ int fx_scan(const uint16_t* __restrict__ idx, const i
     if (s0 + C <= N) {
 #pragma unroll
         for (int j = 0; j < C; ++j) {
-            xv[j] = xo[idx[s0 + j]];
+            xv[j] = fx_round(ro[idx[s0 + j]], fs);
             loc += xv[j];
         }
     } else {
 #pragma unroll
         for (int j = 0; j < C; ++j) {
-            xv[j] = s0 + j < N ? xo[idx[s0 + j]] : 0;
+            xv[j] = s0 + j < N ? fx_round(ro[idx[s0 + j]], fs) : 0;
             loc += xv[j];
         }
     }
@@ -405,10 +392,12 @@ __device__ __forceinline__ float fx_abs_part(const float* __restrict__ ro, int H
     return warp_sum(part);
 }
 
-// Per-card quantities of one scan: twice the prefix at the start of the
-// card's list and the list's mass, one 8-byte load per card.
+// Per-card quantities of one scan, 52 entries each: the scan position of the
+// card's list, twice the prefix at that position, and the list's mass.
 struct FxCards {
-    int2 bm[52];
+    int pos[52];
+    int b2[52];
+    int mass[52];
 };
 
 // One terminal of a unit: where its values go and its payoff scalars.
@@ -430,7 +419,8 @@ struct FxEval {
     const Entry* ent;
     const FxCards* cd;
     const int* X;
-    const int* xo;
+    const float* ro;
+    FxScale fs;
     unsigned Tt;
     int Hq, q;
     bool need_A;
@@ -441,12 +431,13 @@ struct FxEval {
         const Entry et = ent[h];
         if (et.lt == 0xFFFFu) { x.blocked = true; return x; }
         x.live = true;
-        const unsigned ps = et.same >= 0 ? (unsigned)xo[et.same] : 0u;
-        const int2 k1 = cd->bm[et.c1], k2 = cd->bm[et.c2];
-        x.B = Tt - (unsigned)k1.y - (unsigned)k2.y + ps;
+        const unsigned ps = et.same >= 0 ? (unsigned)fx_round(ro[et.same], fs) : 0u;
+        x.B = Tt - (unsigned)cd->mass[et.c1] - (unsigned)cd->mass[et.c2] + ps;
         if (need_A) {
-            x.A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[et.c1lt] - (unsigned)X[et.c1le] -
-                  (unsigned)X[et.c2lt] - (unsigned)X[et.c2le] + (unsigned)k1.x + (unsigned)k2.x + ps;
+            const int s1c = cd->pos[et.c1], s2c = cd->pos[et.c2];
+            x.A = (unsigned)X[et.lt] + (unsigned)X[et.le] - (unsigned)X[s1c + et.ltc1] - (unsigned)X[s1c + et.lec1] -
+                  (unsigned)X[s2c + et.ltc2] - (unsigned)X[s2c + et.lec2] + (unsigned)cd->b2[et.c1] +
+                  (unsigned)cd->b2[et.c2] + ps;
         }
         return x;
     }
@@ -470,16 +461,16 @@ struct FxEval {
 };
 
 // Steps (2)-(4) for player q at a unit of n_it (1 or 2) terminals that share
-// the opponent reach (sibling terminals below a node where q acts: a fold and
-// a call, whose opponent reach is the node's).  xo: that reach in shared
-// memory, already rounded to fixed point with the scale fs of its absolute
-// mass (fx_round_in_place), zero past Ho.  One scan serves the unit: over all
-// three lists if it holds a showdown, else over the per-card lists.
-// X: 3 * Ho + 8 ints; wi: NT / 32.  Ends without a barrier: the caller's next
-// barrier must come before X or xo is written again.
+// the opponent reach ro (sibling terminals below a node where q acts: a fold
+// and a call, whose opponent reach is the node's), staged in shared memory
+// (16-byte aligned, zero past Ho up to a multiple of 4), whose absolute mass
+// S the caller has reduced.  One scan serves the unit: over all three lists
+// if it holds a showdown, else over the per-card lists.  X: 3 * Ho + 8 ints;
+// wi: NT / 32.  Ends without a barrier: the caller's next barrier must come
+// before X or ro is written again.
 template <int NT, int SEM>
 __device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxItem& it1, int n_it, const TabView& tv, int q,
-                                const int* __restrict__ xo, const FxScale& fs, int* X, int* wi, FxCards* cd, int tid) {
+                                const float* __restrict__ ro, float S, int* X, int* wi, FxCards* cd, int tid) {
     static_assert(3 * 1326 <= 17 * NT, "scan chunks of at most 17 positions cover the largest hand count");
     const int o = 1 - q;
     const int Ho = ti.H[o], Hpq = ti.Hp[q];
@@ -487,28 +478,32 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxI
     const int lo = need_A ? 0 : Ho;          // folds alone scan only the per-card lists
     const int N = 3 * Ho - lo;
     const uint16_t* idx = tv.sorted[o] + lo; // [rank order (Ho) | per-card lists (2 Ho)], contiguous
+    const FxScale fs = fx_scale(S);
     const int C = ((N + NT - 1) / NT) | 1;
     int total;
     switch (C) {
-        case 1: total = fx_scan<NT, 1>(idx, xo, N, X, wi, tid); break;
-        case 3: total = fx_scan<NT, 3>(idx, xo, N, X, wi, tid); break;
-        case 5: total = fx_scan<NT, 5>(idx, xo, N, X, wi, tid); break;
-        case 7: total = fx_scan<NT, 7>(idx, xo, N, X, wi, tid); break;
-        case 9: total = fx_scan<NT, 9>(idx, xo, N, X, wi, tid); break;
-        case 11: total = fx_scan<NT, 11>(idx, xo, N, X, wi, tid); break;
-        case 13: total = fx_scan<NT, 13>(idx, xo, N, X, wi, tid); break;
-        case 15: total = fx_scan<NT, 15>(idx, xo, N, X, wi, tid); break;
-        default: total = fx_scan<NT, 17>(idx, xo, N, X, wi, tid); break;
+        case 1: total = fx_scan<NT, 1>(idx, ro, N, fs, X, wi, tid); break;
+        case 3: total = fx_scan<NT, 3>(idx, ro, N, fs, X, wi, tid); break;
+        case 5: total = fx_scan<NT, 5>(idx, ro, N, fs, X, wi, tid); break;
+        case 7: total = fx_scan<NT, 7>(idx, ro, N, fs, X, wi, tid); break;
+        case 9: total = fx_scan<NT, 9>(idx, ro, N, fs, X, wi, tid); break;
+        case 11: total = fx_scan<NT, 11>(idx, ro, N, fs, X, wi, tid); break;
+        case 13: total = fx_scan<NT, 13>(idx, ro, N, fs, X, wi, tid); break;
+        case 15: total = fx_scan<NT, 15>(idx, ro, N, fs, X, wi, tid); break;
+        default: total = fx_scan<NT, 17>(idx, ro, N, fs, X, wi, tid); break;
     }
     const int cb = Ho - lo;                  // scan position of the per-card lists
     if (tid < 52) {
         const uint16_t* seg = tv.seg[o];
-        const int b = X[cb + seg[tid]];
-        cd->bm[tid] = make_int2((int)(2u * (unsigned)b), X[cb + seg[tid + 1]] - b);
+        const int p = cb + seg[tid];
+        const int b = X[p];
+        cd->pos[tid] = p;
+        cd->b2[tid] = (int)(2u * (unsigned)b);
+        cd->mass[tid] = X[cb + seg[tid + 1]] - b;
     }
     __syncthreads();
     FxEval<SEM> ev;
-    ev.ent = tv.ent[q]; ev.cd = cd; ev.X = X; ev.xo = xo;
+    ev.ent = tv.ent[q]; ev.cd = cd; ev.X = X; ev.ro = ro; ev.fs = fs;
     ev.Tt = (unsigned)(need_A ? X[Ho] : total >> 1);   // a fold scan's total is even: exact halving
     ev.Hq = ti.H[q]; ev.q = q; ev.need_A = need_A;
     float ga[2], gc[2], gp[2];
@@ -533,157 +528,6 @@ __device__ void cta_terminal_fx(const TermInfo& ti, const FxItem& it0, const FxI
         if (n_it > 1) {
             out[1][h] = ev.value(x0, fd[1], ga[1], gc[1], gp[1]);
             if (in1) out[1][h + NT] = ev.value(x1, fd[1], ga[1], gc[1], gp[1]);
-        }
-    }
-}
-
-// ---- two units at once ----------------------------------------------------
-// A pair of terminal units with different opponent reach vectors (A and B)
-// valued in one pass: one gather of the scan order feeds both scans (int2
-// elements), and every hand's entry, per-card values and prefix lookups are
-// loaded once for both (8-byte prefix loads, one 16-byte per-card load).
-// Same integer arithmetic per unit as cta_terminal_fx, so the values are
-// bit-identical.
-struct FxCards2 {
-    int4 bm[52];   // per card: b2 and mass of scan A, then of scan B
-};
-
-template <int NT, int C>
-__device__ __forceinline__ int2 fx_scan2(const uint16_t* __restrict__ idx, const int* __restrict__ xa,
-                                         const int* __restrict__ xb, int N, int2* X, int2* wi, int tid) {
-    // pass 1: gather both vectors into this thread's C positions of X and sum
-    // them; pass 2 rewrites the same positions with the exclusive prefix (the
-    // gathered pairs wait in shared memory, not in 2 C registers)
-    const int lane = tid & 31, wid = tid >> 5;
-    const int s0 = min(tid * C, N);
-    int la = 0, lb = 0;
-#pragma unroll
-    for (int j = 0; j < C; ++j) {
-        if (s0 + j < N) {
-            const int k = idx[s0 + j];
-            const int a = xa[k], b = xb[k];
-            X[s0 + j] = make_int2(a, b);
-            la += a;
-            lb += b;
-        }
-    }
-    int ia = la, ib = lb;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int ta = __shfl_up_sync(0xFFFFFFFFu, ia, off);
-        const int tb = __shfl_up_sync(0xFFFFFFFFu, ib, off);
-        if (lane >= off) { ia += ta; ib += tb; }
-    }
-    int ra = ia - la, rb = ib - lb;
-    if (lane == 31) wi[wid] = make_int2(ia, ib);
-    __syncthreads();
-    int2 total = make_int2(0, 0);
-#pragma unroll
-    for (int k = 0; k < NT / 32; ++k) {
-        const int2 w = wi[k];
-        if (k < wid) { ra += w.x; rb += w.y; }
-        total.x += w.x;
-        total.y += w.y;
-    }
-#pragma unroll
-    for (int j = 0; j < C; ++j) {
-        if (s0 + j < N) {
-            const int2 v = X[s0 + j];
-            X[s0 + j] = make_int2(ra, rb);
-            ra += v.x;
-            rb += v.y;
-        }
-    }
-    if (tid == 0) X[N] = total;
-    __syncthreads();
-    return total;
-}
-
-// Values of player q at unit A (nA terminals, opponent reach xa, scale fa)
-// and unit B (nB >= 1 terminals, xb, fb): f0 f1 are unit A's items, f2 f3
-// unit B's (f1 repeats f0 when nA == 1, f3 repeats f2 when nB == 1).
-// X: 3 Ho + 8 int2; wi: NT / 32 int2.  Ends without a barrier, as
-// cta_terminal_fx.
-template <int NT, int SEM>
-__device__ void cta_terminal_fx2(const TermInfo& ti, const FxItem& f0, const FxItem& f1, int nA, const FxItem& f2,
-                                 const FxItem& f3, int nB, const TabView& tv, int q, const int* __restrict__ xa,
-                                 const FxScale& fa, const int* __restrict__ xb, const FxScale& fb, int2* X, int2* wi,
-                                 FxCards2* cd, int tid) {
-    const int o = 1 - q;
-    const int Ho = ti.H[o], Hq = ti.H[q], Hpq = ti.Hp[q];
-    const bool need_A = f0.type != MTT_NODE_FOLD || f1.type != MTT_NODE_FOLD || f2.type != MTT_NODE_FOLD ||
-                        f3.type != MTT_NODE_FOLD;
-    const int lo = need_A ? 0 : Ho;
-    const int N = 3 * Ho - lo;
-    const uint16_t* idx = tv.sorted[o] + lo;
-    const int C = ((N + NT - 1) / NT) | 1;
-    int2 total;
-    switch (C) {
-        case 1: total = fx_scan2<NT, 1>(idx, xa, xb, N, X, wi, tid); break;
-        case 3: total = fx_scan2<NT, 3>(idx, xa, xb, N, X, wi, tid); break;
-        case 5: total = fx_scan2<NT, 5>(idx, xa, xb, N, X, wi, tid); break;
-        case 7: total = fx_scan2<NT, 7>(idx, xa, xb, N, X, wi, tid); break;
-        case 9: total = fx_scan2<NT, 9>(idx, xa, xb, N, X, wi, tid); break;
-        case 11: total = fx_scan2<NT, 11>(idx, xa, xb, N, X, wi, tid); break;
-        case 13: total = fx_scan2<NT, 13>(idx, xa, xb, N, X, wi, tid); break;
-        case 15: total = fx_scan2<NT, 15>(idx, xa, xb, N, X, wi, tid); break;
-        default: total = fx_scan2<NT, 17>(idx, xa, xb, N, X, wi, tid); break;
-    }
-    const int cb = Ho - lo;
-    if (tid < 52) {
-        const uint16_t* seg = tv.seg[o];
-        const int2 b = X[cb + seg[tid]], e = X[cb + seg[tid + 1]];
-        cd->bm[tid] = make_int4((int)(2u * (unsigned)b.x), e.x - b.x, (int)(2u * (unsigned)b.y), e.y - b.y);
-    }
-    __syncthreads();
-    const unsigned TtA = (unsigned)(need_A ? X[Ho].x : total.x >> 1);
-    const unsigned TtB = (unsigned)(need_A ? X[Ho].y : total.y >> 1);
-    // payoff scalars of the (up to) four terminals: A0 A1 B0 B1
-    float ga[4], gc[4], gp[4];
-    bool fd[4];
-    float* out[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const FxItem& it = i == 0 ? f0 : i == 1 ? f1 : i == 2 ? f2 : f3;
-        const FxScale& fs = i < 2 ? fa : fb;
-        const float cq = q ? it.c1 : it.c0;
-        ga[i] = __fmul_rn(__fmul_rn(0.5f, it.pot), fs.inv);
-        gc[i] = __fmul_rn(cq, fs.inv);
-        gp[i] = __fmul_rn((q == ((it.wmask == 1) ? 0 : 1)) ? it.pot - cq : -cq, fs.inv);
-        fd[i] = it.type == MTT_NODE_FOLD;
-        out[i] = (i == 1 && nA < 2) || (i == 3 && nB < 2) ? nullptr : it.out;
-    }
-    const Entry* ent = tv.ent[q];
-    for (int h = tid; h < Hpq; h += NT) {
-        FxHand xA{0u, 0u, false, false}, xB{0u, 0u, false, false};
-        if (h < Hq) {
-            const Entry et = ent[h];
-            if (et.lt == 0xFFFFu) {
-                xA.blocked = xB.blocked = true;
-            } else {
-                xA.live = xB.live = true;
-                const unsigned pa = et.same >= 0 ? (unsigned)xa[et.same] : 0u;
-                const unsigned pb = et.same >= 0 ? (unsigned)xb[et.same] : 0u;
-                const int4 k1 = cd->bm[et.c1], k2 = cd->bm[et.c2];
-                xA.B = TtA - (unsigned)k1.y - (unsigned)k2.y + pa;
-                xB.B = TtB - (unsigned)k1.w - (unsigned)k2.w + pb;
-                if (need_A) {
-                    const int2 a0 = X[et.lt], a1 = X[et.le], a2 = X[et.c1lt], a3 = X[et.c1le], a4 = X[et.c2lt],
-                               a5 = X[et.c2le];
-                    xA.A = (unsigned)a0.x + (unsigned)a1.x - (unsigned)a2.x - (unsigned)a3.x - (unsigned)a4.x -
-                           (unsigned)a5.x + (unsigned)k1.x + (unsigned)k2.x + pa;
-                    xB.A = (unsigned)a0.y + (unsigned)a1.y - (unsigned)a2.y - (unsigned)a3.y - (unsigned)a4.y -
-                           (unsigned)a5.y + (unsigned)k1.z + (unsigned)k2.z + pb;
-                }
-            }
-        }
-        FxEval<SEM> eA, eB;
-        eA.Tt = TtA; eB.Tt = TtB;
-        eA.q = eB.q = q;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            if (!out[i]) continue;
-            out[i][h] = (i < 2 ? eA : eB).value(i < 2 ? xA : xB, fd[i], ga[i], gc[i], gp[i]);
         }
     }
 }
@@ -908,47 +752,30 @@ __host__ __device__ inline int tg_scan_ints(int H0, int H1, int upd) {
     }
     return m;
 }
-// One reach stage: a two-direction launch stages both players' reach of one
-// terminal; a one-direction launch stages the opponent reach of two units
-// (two slots of tg_reach_bytes each).
-__host__ __device__ inline int tg_stage_bytes(int Hp0, int Hp1, int upd) {
-    return upd == 3 ? tg_reach_bytes(Hp0, Hp1, 3) : 2 * tg_reach_bytes(Hp0, Hp1, upd);
-}
-// Scan scratch: int per position for a two-direction launch, int2 (two
-// units at once) for a one-direction launch.
-__host__ __device__ inline int tg_scan_bytes(int H0, int H1, int upd) {
-    return (upd == 3 ? 4 : 8) * tg_scan_ints(H0, H1, upd);
-}
 __host__ __device__ inline int tg_smem_bytes(int H0, int H1, int Hp0, int Hp1, int upd) {
-    return tg_table_bytes(H0, H1, upd) + 2 * tg_stage_bytes(Hp0, Hp1, upd) + tg_scan_bytes(H0, H1, upd) + 16;
+    return tg_table_bytes(H0, H1, upd) + 2 * tg_reach_bytes(Hp0, Hp1, upd) + 4 * tg_scan_ints(H0, H1, upd) + 16;
 }
 
 // Terminal values of the updated players (kernel_evaluate_terminals,
 // honest_multistreet_solver.cu:128-196), one terminal group per CTA.
-// A two-direction launch walks the group's terminals one at a time; a
-// one-direction launch walks it two units at a time (cta_terminal_fx2).
-__global__ void __launch_bounds__(TG, 3) k_term(SolveDev a, const TermGroup* __restrict__ groups,
+__global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __restrict__ groups,
                                              const TermItem* __restrict__ items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s
-    __shared__ float wf[2][2][TG / 32];   // [stage][updated player (two directions) or slot (one)][warp]
-    __shared__ int2 wi2[TG / 32];
+    __shared__ float wf[2][2][TG / 32];   // [terminal parity][updated player][warp]
+    __shared__ int wi[TG / 32];
     __shared__ FxCards cards;
-    __shared__ FxCards2 cards2;
-    int* wi = reinterpret_cast<int*>(wi2);
     const int gi = blockIdx.x, tid = threadIdx.x;
     if (gi >= n) return;
     const TermGroup g = groups[gi];
     const bool both = upd == 3;
     const int q1 = upd == 2 ? 1 : 0;            // the updated player of a one-direction launch
     const uint32_t tb = (uint32_t)tg_table_bytes(g.H0, g.H1, upd);
-    const uint32_t rbytes = (uint32_t)tg_reach_bytes(g.Hp0, g.Hp1, upd);   // one slot (one direction)
-    const uint32_t sbytes = (uint32_t)tg_stage_bytes(g.Hp0, g.Hp1, upd);
+    const uint32_t rbytes = (uint32_t)tg_reach_bytes(g.Hp0, g.Hp1, upd);
     uint8_t* T = smem;
-    float* const Rst0 = reinterpret_cast<float*>(smem + tb);   // stage s starts at Rst0 + s * sbytes / 4
-    void* Xv = smem + tb + 2 * sbytes;   // tb, sbytes: multiples of 16
-    int* X = reinterpret_cast<int*>(Xv);
-    int2* X2 = reinterpret_cast<int2*>(Xv);
+    float* Rst0 = reinterpret_cast<float*>(smem + tb);
+    float* Rst1 = reinterpret_cast<float*>(smem + tb + rbytes);
+    int* X = reinterpret_cast<int*>(smem + tb + 2 * rbytes);   // tb, rbytes: multiples of 16
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -956,47 +783,30 @@ __global__ void __launch_bounds__(TG, 3) k_term(SolveDev a, const TermGroup* __r
         mbar_fence_init();
     }
     __syncthreads();
-    // Steps: a terminal (two directions), or a pair of units (one direction):
-    // unit A = terminals [t, t + lA), unit B = [t + lA, t + lA + lB), lB = 0
-    // when no unit follows.  A unit is a terminal, or two adjacent ones
-    // (siblings) whose opponent reach for the updated player is the same vector.
-    const int o1 = 1 - q1;
-    auto unit_len = [&](int t) -> int {
-        if (t + 1 >= g.count) return 1;
-        return items[g.first + t + 1].ro[o1] == items[g.first + t].ro[o1] ? 2 : 1;
-    };
-    auto step_at = [&](int t, int& lA, int& lB) {
-        if (both) { lA = 1; lB = 0; return; }
-        lA = unit_len(t);
-        lB = t + lA < g.count ? unit_len(t + lA) : 0;
-    };
-    // thread 0 issues every copy
-    auto issue_step = [&](int t, int lA, int lB, int s) {
+    // thread 0 issues every copy; stage s of terminal t is reach vector(s) of items[first + t]
+    auto issue_reach = [&](int t, int s) {
         const TermItem& it = items[g.first + t];
-        float* dst = Rst0 + s * (sbytes >> 2);
+        float* dst = s ? Rst1 : Rst0;
+        mbar_arrive_expect_tx(&bar[1 + s], rbytes);
         if (both) {
-            mbar_arrive_expect_tx(&bar[1 + s], sbytes);
             bulk_g2s(dst, a.arena + it.ro[0], 4u * (uint32_t)g.Hp0, &bar[1 + s]);
             bulk_g2s(dst + g.Hp0, a.arena + it.ro[1], 4u * (uint32_t)g.Hp1, &bar[1 + s]);
         } else {
-            mbar_arrive_expect_tx(&bar[1 + s], lB ? 2 * rbytes : rbytes);
-            bulk_g2s(dst, a.arena + it.ro[o1], rbytes, &bar[1 + s]);
-            if (lB) bulk_g2s(dst + rbytes / 4, a.arena + items[g.first + t + lA].ro[o1], rbytes, &bar[1 + s]);
+            bulk_g2s(dst, a.arena + it.ro[1 - q1], rbytes, &bar[1 + s]);
         }
     };
-    int t = 0, lA = 1, lB = 0;
-    step_at(0, lA, lB);
     if (tid == 0) {
         mbar_arrive_expect_tx(&bar[0], tb);
         if (both) {
             bulk_g2s(T, a.tabs + g.tab, tb, &bar[0]);
         } else {
-            const int Ho = o1 ? g.H1 : g.H0;
+            const int o = 1 - q1;
+            const int Ho = o ? g.H1 : g.H0;
             const uint32_t ib = (uint32_t)tab_idx_bytes(Ho);
-            bulk_g2s(T, a.tabs + g.tab + tab_idx_off(o1, g.H0), ib, &bar[0]);
+            bulk_g2s(T, a.tabs + g.tab + tab_idx_off(o, g.H0), ib, &bar[0]);
             bulk_g2s(T + ib, a.tabs + g.tab + tab_ent_off(q1, g.H0, g.H1), tb - ib, &bar[0]);
         }
-        issue_step(0, lA, lB, 0);
+        issue_reach(0, 0);
     }
     const bool okt = mbar_wait_bounded(&bar[0], 0u);
     if (__syncthreads_or(!okt)) {
@@ -1021,117 +831,77 @@ __global__ void __launch_bounds__(TG, 3) k_term(SolveDev a, const TermGroup* __r
     }
     TermInfo ti;
     ti.H[0] = g.H0; ti.H[1] = g.H1; ti.Hp[0] = g.Hp0; ti.Hp[1] = g.Hp1;
-    const int Hpo1 = o1 ? g.Hp1 : g.Hp0;       // padded opponent count (one direction)
-    // vector v of a stage: two directions, player v's reach (the opponent
-    // reach of player 1 - v); one direction, slot v
-    auto vec = [&](int s, int v) -> float* {
-        float* st = Rst0 + s * (sbytes >> 2);
-        return both ? (v == 0 ? st : st + g.Hp0) : st + v * Hpo1;
-    };
-    // absolute masses of a stage's vectors into wf[s][slot]; read after the next barrier
-    auto mass_parts = [&](int s, int nvec) {
-        if (both) {
+    // opponent reach of player q inside a stage: player 1's part follows
+    // player 0's in a two-direction stage
+    auto opp = [&](const float* st, int q) -> const float* { return both ? (q == 0 ? st + g.Hp0 : st) : st; };
+    // absolute opponent masses of the terminal staged in st, per updated
+    // player, into wf[buf]; read after the next barrier
+    auto mass_parts = [&](const float* st, int buf) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const float p = fx_abs_part<TG>(vec(s, 1 - q), q ? g.H0 : g.H1, tid);
-                if ((tid & 31) == 0) wf[s][q][tid >> 5] = p;
-            }
-        } else {
-            const int Ho = q1 ? g.H0 : g.H1;
-            for (int v = 0; v < nvec; ++v) {
-                const float p = fx_abs_part<TG>(vec(s, v), Ho, tid);
-                if ((tid & 31) == 0) wf[s][v][tid >> 5] = p;
-            }
+        for (int q = 0; q < 2; ++q) {
+            if (!((upd >> q) & 1)) continue;
+            const float p = fx_abs_part<TG>(opp(st, q), q ? g.H0 : g.H1, tid);
+            if ((tid & 31) == 0) wf[buf][q][tid >> 5] = p;
         }
-    };
-    auto mass = [&](int s, int v) {
-        float S = 0.f;
-#pragma unroll
-        for (int k = 0; k < TG / 32; ++k) S += wf[s][v][k];
-        return S;
-    };
-    auto load_item = [&](FxItem& f, const TermItem& it, int q) {
-        f.pot = it.pot; f.c0 = it.c0; f.c1 = it.c1;
-        f.type = it.type_wmask & 0xFF; f.wmask = (it.type_wmask >> 8) & 0xFF;
-        f.out = a.arena + it.out[q];
     };
     uint32_t parity = 1u;   // bit s: phase of stage s's next wait (stage 0's first is done below)
     {
         const bool ok = mbar_wait_bounded(&bar[1], 0u);
-        if (ok) mass_parts(0, lB ? 2 : 1);
+        if (ok) mass_parts(Rst0, 0);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(a.err, 1);
             return;
         }
     }
+    // Units: a terminal, or two adjacent ones (siblings) whose opponent reach
+    // for the updated player is the same vector (one direction only).
+    auto unit_len = [&](int t) -> int {
+        if (both || t + 1 >= g.count) return 1;
+        const int o = 1 - q1;
+        return items[g.first + t + 1].ro[o] == items[g.first + t].ro[o] ? 2 : 1;
+    };
+    int t = 0, len = unit_len(0);
     for (int u = 0; t < g.count; ++u) {
         const int s = u & 1;
-        const int tn = t + lA + lB;              // the next step's first terminal
-        int nA = 1, nB = 0;
-        if (tn < g.count) step_at(tn, nA, nB);
-        // stage s ^ 1 was last read by the previous step, which ended on a barrier
-        if (tid == 0 && tn < g.count) issue_step(tn, nA, nB, s ^ 1);
-        if (both) {
-            // each player's opponent reach, rounded in place with its own scale
-            FxScale fs[2];
+        const int tn = t + len;                  // the next unit's first terminal
+        // stage s ^ 1 was last read by the previous unit, which ended on a barrier
+        if (tid == 0 && tn < g.count) issue_reach(tn, s ^ 1);
+        FxItem f0, f1;
+        auto load_item = [&](FxItem& f, const TermItem& it) {
+            f.pot = it.pot; f.c0 = it.c0; f.c1 = it.c1;
+            f.type = it.type_wmask & 0xFF; f.wmask = (it.type_wmask >> 8) & 0xFF;
+        };
+        const TermItem& ia = items[g.first + t];
+        const TermItem& ib = items[g.first + t + (len > 1 ? 1 : 0)];
+        load_item(f0, ia);
+        load_item(f1, ib);
+        const float* st = s ? Rst1 : Rst0;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                fs[q] = fx_scale(mass(s, q));
-                fx_round_in_place<TG>(vec(s, 1 - q), (q ? g.Hp0 : g.Hp1) >> 2, fs[q], tid);
-            }
-            __syncthreads();
-            const TermItem& it = items[g.first + t];
+        for (int q = 0; q < 2; ++q) {
+            if (!((upd >> q) & 1)) continue;
+            float S = 0.f;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                FxItem f;
-                load_item(f, it, q);
-                if (q == 1) __syncthreads();   // player 0's values have been read out of X
-                const int* xo = reinterpret_cast<const int*>(vec(s, 1 - q));
-                if (a.semantics) cta_terminal_fx<TG, MTT_SEM_REFERENCE>(ti, f, f, 1, tv, q, xo, fs[q], X, wi, &cards, tid);
-                else cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, f, f, 1, tv, q, xo, fs[q], X, wi, &cards, tid);
-            }
-        } else {
-            // A's items, then B's (a missing second item repeats the first)
-            FxItem f0, f1, f2, f3;
-            load_item(f0, items[g.first + t], q1);
-            load_item(f1, items[g.first + t + (lA > 1 ? 1 : 0)], q1);
-            load_item(f2, items[g.first + t + (lB ? lA : 0)], q1);
-            load_item(f3, items[g.first + t + (lB ? lA + (lB > 1 ? 1 : 0) : 0)], q1);
-            const FxScale sa = fx_scale(mass(s, 0));
-            const FxScale sb = lB ? fx_scale(mass(s, 1)) : sa;
-            fx_round_in_place<TG>(vec(s, 0), Hpo1 >> 2, sa, tid);
-            if (lB) fx_round_in_place<TG>(vec(s, 1), Hpo1 >> 2, sb, tid);
-            __syncthreads();
-            const int* xa = reinterpret_cast<const int*>(vec(s, 0));
-            const int* xb = reinterpret_cast<const int*>(vec(s, 1));
-            if (lB) {
-                if (a.semantics)
-                    cta_terminal_fx2<TG, MTT_SEM_REFERENCE>(ti, f0, f1, lA, f2, f3, lB, tv, q1, xa, sa, xb, sb, X2, wi2,
-                                                            &cards2, tid);
-                else
-                    cta_terminal_fx2<TG, MTT_SEM_CORRECT>(ti, f0, f1, lA, f2, f3, lB, tv, q1, xa, sa, xb, sb, X2, wi2,
-                                                          &cards2, tid);
-            } else {
-                if (a.semantics)
-                    cta_terminal_fx<TG, MTT_SEM_REFERENCE>(ti, f0, f1, lA, tv, q1, xa, sa, X, wi, &cards, tid);
-                else
-                    cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, f0, f1, lA, tv, q1, xa, sa, X, wi, &cards, tid);
-            }
+            for (int k = 0; k < TG / 32; ++k) S += wf[s][q][k];
+            f0.out = a.arena + ia.out[q];
+            f1.out = a.arena + ib.out[q];
+            if (both && q == 1) __syncthreads();   // player 0's values have been read out of X
+            if (a.semantics) cta_terminal_fx<TG, MTT_SEM_REFERENCE>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, tid);
+            else cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, f0, f1, len, tv, q, opp(st, q), S, X, wi, &cards, tid);
         }
-        // the next step's reach and masses; the barrier also ends this step
+        // the next unit's reach and masses; the barrier also ends this unit
+        const int lenn = tn < g.count ? unit_len(tn) : 0;
         bool ok = true;
         if (tn < g.count) {
             ok = mbar_wait_bounded(&bar[2 - s], (parity >> (s ^ 1)) & 1u);
             parity ^= 1u << (s ^ 1);
-            if (ok) mass_parts(s ^ 1, nB ? 2 : 1);
+            if (ok) mass_parts(s ? Rst0 : Rst1, s ^ 1);
         }
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(a.err, 1);
             return;
         }
         t = tn;
-        lA = nA;
-        lB = nB;
+        len = lenn;
     }
 }
 
@@ -1387,9 +1157,6 @@ __global__ void __launch_bounds__(TG) k_leaf_showdown(SolveDev a, const LeafItem
         float S = 0.0f;
 #pragma unroll
         for (int k = 0; k < TG / 32; ++k) S += wf[k];
-        const FxScale fs = fx_scale(S);
-        fx_round_in_place<TG>(ro, L.Hp[o] >> 2, fs, tid);
-        __syncthreads();
         TabView tv;
         const uint16_t *so, *co, *sg;
         tab_idx_view(T, Ho, &so, &co, &sg);
@@ -1403,8 +1170,7 @@ __global__ void __launch_bounds__(TG) k_leaf_showdown(SolveDev a, const LeafItem
         it.out = SD + ((size_t)row * 2 + q) * sd_stride;
         it.pot = L.pot; it.c0 = 0.5f * L.pot; it.c1 = 0.5f * L.pot;
         it.type = MTT_NODE_SHOWDOWN; it.wmask = 3;
-        cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, it, it, 1, tv, q, reinterpret_cast<const int*>(ro), fs, X, wi, &cards,
-                                             tid);
+        cta_terminal_fx<TG, MTT_SEM_CORRECT>(ti, it, it, 1, tv, q, ro, S, X, wi, &cards, tid);
         __syncthreads();   // the next player restages shared memory
     }
 }

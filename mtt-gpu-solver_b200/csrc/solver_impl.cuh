@@ -60,20 +60,16 @@ struct alignas(16) SubDesc {
 //   IDX0 = u16 sorted0[H0] | u16 cl0[2*H0] | u16 seg0[54]      (opponent lists of player 0)
 //   IDX1 = the same for player 1
 //   ENT0 = Entry e0[H0] (player-0 hands against player-1 lists), ENT1 = Entry e1[H1]
-// One hand against the opponent's lists, 16 bytes (one shared-memory load).
-// Positions index the scan [opponent rank order (Ho) | opponent per-card
-// lists (2 Ho)]: lt / le, the first opponent hand ranked >= / > this hand in
-// rank order; c1lt / c1le (c2lt / c2le), the same inside the list of opponent
-// hands holding this hand's first (second) card, as absolute scan positions
-// (Ho + start of that card's list + rank offset inside it).
-struct alignas(16) Entry {
-    uint16_t lt, le;       // lt == 0xFFFF: hand blocked by the dealt card
-    uint16_t c1lt, c1le;
-    uint16_t c2lt, c2le;
-    uint8_t c1, c2;
-    int16_t same;          // opponent index of the same combo, -1 if absent
+// One hand against the opponent's lists.  lt / le: position in the
+// opponent's rank order of the first hand ranked >= / > this hand;
+// ltc1 / lec1 (ltc2 / lec2): the same inside the list of opponent hands
+// holding this hand's first (second) card.
+struct alignas(4) Entry {
+    uint8_t c1, c2, ltc1, lec1, ltc2, lec2;
+    uint16_t lt, le;     // lt == 0xFFFF: hand blocked by the dealt card
+    int16_t same;        // opponent index of the same combo, -1 if absent
 };
-static_assert(sizeof(Entry) == 16, "Entry is 16 bytes");
+static_assert(sizeof(Entry) == 12, "Entry is 12 bytes");
 
 struct TabView {
     const uint16_t* sorted[2];
@@ -84,7 +80,7 @@ struct TabView {
 
 __host__ __device__ inline int round16(int b) { return (b + 15) & ~15; }
 __host__ __device__ inline int tab_idx_bytes(int H) { return round16(2 * (3 * H + 54)); }
-__host__ __device__ inline int tab_ent_bytes(int H) { return 16 * H; }
+__host__ __device__ inline int tab_ent_bytes(int H) { return round16(12 * H); }
 __host__ __device__ inline int tab_idx_off(int p, int H0) { return p ? tab_idx_bytes(H0) : 0; }
 __host__ __device__ inline int tab_ent_off(int p, int H0, int H1) {
     return tab_idx_bytes(H0) + tab_idx_bytes(H1) + (p ? tab_ent_bytes(H0) : 0);

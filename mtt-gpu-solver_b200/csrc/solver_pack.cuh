@@ -84,16 +84,14 @@ static void build_variant(const uint8_t* board, int nboard, int dealt, const int
             const uint32_t s = sc[q][h];
             e.lt = (uint16_t)(std::lower_bound(ssc[o].begin(), ssc[o].end(), s) - ssc[o].begin());
             e.le = (uint16_t)(std::upper_bound(ssc[o].begin(), ssc[o].end(), s) - ssc[o].begin());
-            // absolute positions in the scan [rank order (H_o) | per-card lists (2 H_o)]
             auto seg_pos = [&](int c, bool upper) {
                 auto b = clsc[o].begin() + seg[o][c], en = clsc[o].begin() + seg[o][c + 1];
-                const long k = (upper ? std::upper_bound(b, en, s) : std::lower_bound(b, en, s)) - clsc[o].begin();
-                return (uint16_t)(H[o] + k);
+                return (uint8_t)((upper ? std::upper_bound(b, en, s) : std::lower_bound(b, en, s)) - b);
             };
-            e.c1lt = seg_pos(c1, false);
-            e.c1le = seg_pos(c1, true);
-            e.c2lt = seg_pos(c2, false);
-            e.c2le = seg_pos(c2, true);
+            e.ltc1 = seg_pos(c1, false);
+            e.lec1 = seg_pos(c1, true);
+            e.ltc2 = seg_pos(c2, false);
+            e.lec2 = seg_pos(c2, true);
             const uint16_t cid = combos[q][h];
             auto it = std::lower_bound(combos[o].begin(), combos[o].end(), cid);
             e.same = (it != combos[o].end() && *it == cid) ? (int16_t)(it - combos[o].begin()) : (int16_t)-1;

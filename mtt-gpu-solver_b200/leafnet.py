@@ -219,24 +219,50 @@ def checkdown_values_fp64(meta, batch=4096):
 
 def gemm_timing(M=4096, N=1024, K=2752, reps=20, seed=0):
     """Device time of the leaf network's tcgen05 GEMM on one shape
-    (C[M x N] fp32 = A[M x K] B[N x K]^T, bf16 operands): (ms per call,
-    TFLOP/s), CUDA events on the current stream after one warm-up call."""
+    (C[M x N] fp32 = A[M x K] B[N x K]^T, bf16 operands), two ways, after a
+    warm-up call, with CUDA events on the current stream:
+    - per call: reps calls from Python, each launched by the library (host
+      work between launches included);
+    - graph: the same reps launches captured once in a CUDA graph and
+      replayed (the kernels back to back).
+    Returns {"call_ms", "graph_ms", "call_tflops", "graph_tflops"}."""
     import torch
     from . import gemm_bf16
     g = torch.Generator(device="cuda").manual_seed(seed)
     A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
     C = torch.empty(M, N, device="cuda")
-    gemm_bf16(A, B, out=C)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")   # one error word, checked at the end
+    gemm_bf16(A, B, out=C, err=err)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
     for _ in range(reps):
-        gemm_bf16(A, B, out=C)
+        gemm_bf16(A, B, out=C, err=err)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    return ms, 2.0 * M * N * K / (ms * 1e-3) / 1e12
+    call_ms = e0.elapsed_time(e1) / reps
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        gemm_bf16(A, B, out=C, err=err, stream=s)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=s):
+            for _ in range(reps):
+                gemm_bf16(A, B, out=C, err=err, stream=s)
+    graph.replay()
+    torch.cuda.synchronize()
+    e0.record()
+    graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1) / reps
+    if int(err.item()):
+        raise RuntimeError("a bounded wait in the GEMM gave up")
+    fl = 2.0 * M * N * K
+    return {"call_ms": call_ms, "graph_ms": graph_ms, "call_tflops": fl / (call_ms * 1e-3) / 1e12,
+            "graph_tflops": fl / (graph_ms * 1e-3) / 1e12}
 
 
 if __name__ == "__main__":
@@ -245,5 +271,6 @@ if __name__ == "__main__":
     ap.add_argument("--shape", type=int, nargs=3, default=[4096, 1024, 2752], metavar=("M", "N", "K"))
     ap.add_argument("--reps", type=int, default=20)
     a = ap.parse_args()
-    ms, tf = gemm_timing(*a.shape, reps=a.reps)
-    print(f"gemm {a.shape[0]}x{a.shape[1]}x{a.shape[2]}: {ms:.4f} ms, {tf:.1f} TFLOP/s")
+    t = gemm_timing(*a.shape, reps=a.reps)
+    print(f"gemm {a.shape[0]}x{a.shape[1]}x{a.shape[2]}: per call {t['call_ms']:.4f} ms ({t['call_tflops']:.1f} "
+          f"TFLOP/s), graph-replayed {t['graph_ms']:.4f} ms ({t['graph_tflops']:.1f} TFLOP/s)")
