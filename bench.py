@@ -30,11 +30,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "batched river solves/s at <=0.1% pot exploitability vs plain kernel; evals/s"
 # DRAM bytes (read + write) of one CFR iteration of the sweeps and terminals
-# (k_fwd x6, k_term x6, k_bwd x12) on the default workload (4096 subgames,
-# seed 2), from a one-pass ncu capture of dram__bytes_read.sum +
-# dram__bytes_write.sum over 26 complete iterations (min 13.435, max 13.498 GB);
-# the algorithmic bytes of the same iteration are 14.251 GB.
-TRAFFIC_PER_ITER = {"subgames": 4096, "seed": 2, "bytes": 13.484e9}
+# from a one-kernel-class-at-a-time ncu capture of a 256-subgame batch (seed 2;
+# 4.5 iterations, 650.5 MB per iteration against 977.6 MB of algorithmic bytes).
+# The bench scales it by the subgame count; at 256 subgames part of the round
+# trips stays in L2, so the scaled figure is a lower bound.
+TRAFFIC_PER_ITER = {"subgames": 256, "seed": 2, "bytes": 650.48e6}
 
 
 def parse():
@@ -490,8 +490,8 @@ def run_b200(args, rank, world, local):
     solve_ms = k0.elapsed_time(k1)
     algo_bytes = info["iter_bytes"] * args.iters
     achieved = algo_bytes / (solve_ms * 1e-3) / 1e9
-    traffic = (TRAFFIC_PER_ITER["bytes"] if (args.subgames, args.seed) ==
-               (TRAFFIC_PER_ITER["subgames"], TRAFFIC_PER_ITER["seed"]) else None)
+    traffic = (TRAFFIC_PER_ITER["bytes"] * args.subgames / TRAFFIC_PER_ITER["subgames"]
+               if args.seed == TRAFFIC_PER_ITER["seed"] else None)
     peak, peak_kind = load_peaks()
     # per kernel class: CUDA events around each class in every pass (level
     # launches without the graph), compulsory bytes from the work lists
@@ -602,7 +602,9 @@ def run_b200(args, rank, world, local):
             "reference_kernels": ref_kernels,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "traffic_unit": "DRAM bytes per CFR iteration (ncu capture of this workload)",
+                         "traffic_unit": "DRAM bytes per CFR iteration: ncu capture of a 256-subgame batch scaled "
+                                         "by the subgame count (a lower bound: part of the small batch's round "
+                                         "trips stays in L2)",
                          "algorithmic_bytes_per_iter": int(info["iter_bytes"]),
                          "kernel": "CFR sweeps + terminals (k_fwd, k_term, k_bwd), no best response",
                          "peak_kind": peak_kind, "kernel_ms": solve_ms, "per_kernel": kernels},
