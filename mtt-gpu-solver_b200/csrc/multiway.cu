@@ -519,17 +519,24 @@ __global__ void __launch_bounds__(MT) k_mw_term(MwDev a, const int2* __restrict_
     }
 }
 
-// The correct semantics' terminal, one terminal per CTA: every player's
-// reach gathered into [rank order | per-card lists in rank order] (3 H
-// positions) and scanned (exclusive, FP64); per hero hand h and opponent o,
-// the masses below, equal to and in total over o's hands that share no card
-// with h are differences of that scan (as in the heads-up terminals: the
-// per-card lists of h's two cards are subtracted, the combo h itself, counted
-// in both, added back once).
+// The correct semantics' terminal, one terminal per CTA.  Each player's reach
+// at the terminal is staged in shared memory (coalesced), scaled by a power of
+// two 2^k_o with S_o 2^k_o < 2^29 for its absolute mass S_o and rounded to
+// int32, then gathered into [rank order | per-card lists in rank order] (3 H
+// positions) and scanned exclusively in integers.  Per hero hand h and
+// opponent o, the masses of o's hands that share no card with h, ranked below
+// (L), equal (E) and in total (W), are integer differences of that scan (the
+// heads-up terminals' construction: the per-card lists of h's two cards are
+// subtracted, the combo h itself, counted in both, added back once), exact
+// and independent of the summation order, so a mass that is zero stays zero.
+// Every prefix is below 3 (2^29 + H / 2) < 2^31; each reach value is off by at
+// most 2^-30 S_o.  The payoffs are then formed in FP64.
 __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
-    extern __shared__ __align__(16) double xs[];     // [NP][3 H + 1]
-    __shared__ double wb[MT / 32];
-    __shared__ double2 ct[NP][52];                   // per player and card: scan at the list start, list mass
+    extern __shared__ __align__(16) int xsi[];       // [NP][3 H + 1] scans, then [NP][Hp] staged reach
+    __shared__ int wbi[MT / 32];
+    __shared__ float wsum[NP][MT / 32];
+    __shared__ int2 ct[NP][52];                      // per player and card: scan at the list start, list mass
+    __shared__ double inv_s[NP];                     // 2^-k_o
     const int t = blockIdx.x, tid = threadIdx.x;
     if (t >= n) return;
     const int node = terms[t].x, sub = terms[t].y;
@@ -541,38 +548,69 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     const MwEntry* ent = reinterpret_cast<const MwEntry*>(a.tabs + d.cent_base);
     const long long HS = (long long)NP * Hp;
     const int k_local = node - (int)d.node_base;
-    const float* ro[NP];
+    float* rf = reinterpret_cast<float*>(xsi + NP * X);   // [NP][Hp] floats, then the same words as int
+    int* ri = xsi + NP * X;
+    const int lane = tid & 31, wid = tid >> 5;
+    // stage every player's reach (float4, coalesced) and its absolute mass
+    for (int o = 0; o < NP; ++o) {
+        const float4* src = reinterpret_cast<const float4*>(a.arena + d.arena_base + (long long)nd.src[o] * HS +
+                                                            (long long)o * Hp);
+        float4* dst = reinterpret_cast<float4*>(rf + o * Hp);
+        float part = 0.f;
+        for (int j = tid; j < (Hp >> 2); j += MT) {
+            float4 v = src[j];
+            const int h0 = 4 * j;
+            if (h0 + 0 >= H) v.x = 0.f;
+            if (h0 + 1 >= H) v.y = 0.f;
+            if (h0 + 2 >= H) v.z = 0.f;
+            if (h0 + 3 >= H) v.w = 0.f;
+            dst[j] = v;
+            part += (fabsf(v.x) + fabsf(v.y)) + (fabsf(v.z) + fabsf(v.w));
+        }
 #pragma unroll
-    for (int o = 0; o < NP; ++o) ro[o] = a.arena + d.arena_base + (long long)nd.src[o] * HS + (long long)o * Hp;
+        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, off);
+        if (lane == 0) wsum[o][wid] = part;
+    }
+    __syncthreads();
+    // the power-of-two scale of each player and the rounding to int32, in place
+    for (int o = 0; o < NP; ++o) {
+        float S = 0.f;
+#pragma unroll
+        for (int k = 0; k < MT / 32; ++k) S += wsum[o][k];
+        const int E = (int)((__float_as_uint(S) >> 23) & 0xFFu);
+        const int e = E == 0 ? -126 : E - 126;                       // S < 2^e
+        const int kk = S > 0.f ? min(max(29 - e, -126), 126) : 0;
+        const float f = __uint_as_float((uint32_t)(127 + kk) << 23);
+        if (tid == 0) inv_s[o] = (double)__uint_as_float((uint32_t)(127 - kk) << 23);
+        for (int j = tid; j < Hp; j += MT) ri[o * Hp + j] = __float2int_rn(__fmul_rn(rf[o * Hp + j], f));
+    }
+    __syncthreads();
     for (int o = 0; o < NP; ++o)
-        for (int k = tid; k < N; k += MT) xs[o * X + k] = (double)ro[o][idx[k]];
+        for (int k = tid; k < N; k += MT) xsi[o * X + k] = ri[o * Hp + idx[k]];
     __syncthreads();
     const int C = (N + MT - 1) / MT;
     const int s0 = min(tid * C, N), s1 = min(s0 + C, N);
-    const int lane = tid & 31, wid = tid >> 5;
     for (int o = 0; o < NP; ++o) {
-        double* x = xs + o * X;
-        double loc = 0.0;
+        int* x = xsi + o * X;
+        int loc = 0;
         for (int k = s0; k < s1; ++k) loc += x[k];
-        double inc = loc;
+        int inc = loc;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-            const double v = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+            const int v = __shfl_up_sync(0xFFFFFFFFu, inc, off);
             if (lane >= off) inc += v;
         }
-        double run = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-        if (lane == 0) run = 0.0;
-        if (lane == 31) wb[wid] = inc;
+        int run = inc - loc;
+        if (lane == 31) wbi[wid] = inc;
         __syncthreads();
-        double base = 0.0, total = 0.0;
+        int total = 0;
 #pragma unroll
         for (int k = 0; k < MT / 32; ++k) {
-            if (k < wid) base += wb[k];
-            total += wb[k];
+            if (k < wid) run += wbi[k];
+            total += wbi[k];
         }
-        run += base;
         for (int k = s0; k < s1; ++k) {
-            const double v = x[k];
+            const int v = x[k];
             x[k] = run;
             run += v;
         }
@@ -581,8 +619,8 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     }
     for (int i = tid; i < NP * 52; i += MT) {
         const int o = i / 52, c = i - 52 * o;
-        const double b0 = xs[o * X + H + seg[c]];
-        ct[o][c] = make_double2(b0, xs[o * X + H + seg[c + 1]] - b0);
+        const int b0 = xsi[o * X + H + seg[c]];
+        ct[o][c] = make_int2(b0, (int)((unsigned)xsi[o * X + H + seg[c + 1]] - (unsigned)b0));
     }
     __syncthreads();
     const int am = nd.amask;
@@ -593,12 +631,18 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
             const MwEntry e = ent[h];
 #pragma unroll
             for (int o = 0; o < NP; ++o) {
-                const double* x = xs + o * X;
-                const double2 k1 = ct[o][e.c1], k2 = ct[o][e.c2];
-                const double rh = (double)ro[o][h];
-                L[o] = x[e.lt] - (x[e.c1lt] - k1.x) - (x[e.c2lt] - k2.x);
-                E[o] = x[e.le] - (x[e.c1le] - k1.x) - (x[e.c2le] - k2.x) + rh - L[o];
-                W[o] = x[H] - k1.y - k2.y + rh;
+                const int* x = xsi + o * X;
+                const int2 k1 = ct[o][e.c1], k2 = ct[o][e.c2];
+                const unsigned rh = (unsigned)ri[o * Hp + h];
+                const unsigned l = (unsigned)x[e.lt] - ((unsigned)x[e.c1lt] - (unsigned)k1.x) -
+                                   ((unsigned)x[e.c2lt] - (unsigned)k2.x);
+                const unsigned le = (unsigned)x[e.le] - ((unsigned)x[e.c1le] - (unsigned)k1.x) -
+                                    ((unsigned)x[e.c2le] - (unsigned)k2.x) + rh;
+                const unsigned w = (unsigned)x[H] - (unsigned)k1.y - (unsigned)k2.y + rh;
+                const double sc = inv_s[o];
+                L[o] = (double)(int)l * sc;
+                E[o] = (double)(int)(le - l) * sc;
+                W[o] = (double)(int)w * sc;
             }
         }
         for (int p = 0; p < NP; ++p) {
@@ -702,8 +746,11 @@ void free_mw(mtt_mw_batch* b) {
     delete b;
 }
 
-// Dynamic shared memory of k_mw_term_cr: four scans of 3 H + 1 doubles.
-size_t term_cr_smem(const mtt_mw_batch* b) { return sizeof(double) * (size_t)NP * (3 * (size_t)b->Hmax + 1); }
+// Dynamic shared memory of k_mw_term_cr: four int32 scans of 3 H + 1
+// positions and the four staged reach vectors.
+size_t term_cr_smem(const mtt_mw_batch* b) {
+    return sizeof(int) * (size_t)NP * (3 * (size_t)b->Hmax + 1) + sizeof(float) * (size_t)NP * (size_t)b->Hmax + 16;
+}
 
 MwDev mw_args(const mtt_mw_batch* b, int algo, int sem) {
     MwDev a;
