@@ -717,7 +717,8 @@ __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __res
 // Terminals are processed in groups: consecutive terminals of one subgame
 // that share a showdown table variant (all of a river subgame's terminals,
 // or those below one river card of a turn subgame), at most TG_CHUNK per
-// CTA.  The CTA stages the table blocks once, then walks its terminals with
+// CTA.  The CTA stages the table blocks and the group's work items once, then
+// walks its terminals with
 // the opponent reach of terminal t+1 in flight (1-D bulk copy on the other
 // stage's mbarrier) while terminal t is evaluated from shared memory.
 constexpr int TG = 256;         // threads per terminal-group CTA (fixed: the scan chunks depend on it)
@@ -759,15 +760,18 @@ __host__ __device__ inline int tg_smem_bytes(int H0, int H1, int Hp0, int Hp1, i
 // Terminal values of the updated players (kernel_evaluate_terminals,
 // honest_multistreet_solver.cu:128-196), one terminal group per CTA.
 __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __restrict__ groups,
-                                             const TermItem* __restrict__ items, int n, int upd) {
+                                             const TermItem* items, int n, int upd) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[3];   // 0: table blocks, 1 + s: reach stage s
     __shared__ float wf[2][2][TG / 32];   // [terminal parity][updated player][warp]
     __shared__ int wi[TG / 32];
     __shared__ FxCards cards;
+    __shared__ __align__(16) TermItem sitems[TG_CHUNK];   // the group's items, staged with the table
     const int gi = blockIdx.x, tid = threadIdx.x;
     if (gi >= n) return;
     const TermGroup g = groups[gi];
+    const TermItem* const gitems = items;
+    items = sitems - g.first;      // items[g.first + t] reads the staged copy below
     const bool both = upd == 3;
     const int q1 = upd == 2 ? 1 : 0;            // the updated player of a one-direction launch
     const uint32_t tb = (uint32_t)tg_table_bytes(g.H0, g.H1, upd);
@@ -785,7 +789,7 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
     __syncthreads();
     // thread 0 issues every copy; stage s of terminal t is reach vector(s) of items[first + t]
     auto issue_reach = [&](int t, int s) {
-        const TermItem& it = items[g.first + t];
+        const TermItem& it = gitems[g.first + t];   // the first one is issued before the staged copy lands
         float* dst = s ? Rst1 : Rst0;
         mbar_arrive_expect_tx(&bar[1 + s], rbytes);
         if (both) {
@@ -796,7 +800,8 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
         }
     };
     if (tid == 0) {
-        mbar_arrive_expect_tx(&bar[0], tb);
+        mbar_arrive_expect_tx(&bar[0], tb + (uint32_t)(sizeof(TermItem) * g.count));
+        bulk_g2s(sitems, gitems + g.first, (uint32_t)(sizeof(TermItem) * g.count), &bar[0]);
         if (both) {
             bulk_g2s(T, a.tabs + g.tab, tb, &bar[0]);
         } else {
