@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(MT) k_mw_term(MwDev a, const int2* __restrict_
 // and independent of the summation order, so a mass that is zero stays zero.
 // Every prefix is below 3 (2^29 + H / 2) < 2^31; each reach value is off by at
 // most 2^-30 S_o.  The payoffs are then formed in FP64.
-__global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
+__global__ void __launch_bounds__(MT, 3) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
     extern __shared__ __align__(16) int xsi[];       // [NP][3 H + 1] scans, then [NP][Hp] staged reach
     __shared__ int wbi[MT / 32];
     __shared__ float wsum[NP][MT / 32];
@@ -624,9 +624,14 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     }
     __syncthreads();
     const int am = nd.amask;
+    const bool fold = nd.type == MTT_NODE_FOLD;
+    const int winner = __ffs(am) - 1;
+    const double pot = (double)nd.pot;
     float* outb = a.arena + d.arena_base + (long long)d.n_nodes * HS + (long long)k_local * HS;
     for (int h = tid; h < Hp; h += MT) {
         double L[NP], E[NP], W[NP];
+#pragma unroll
+        for (int o = 0; o < NP; ++o) { L[o] = 0.0; E[o] = 0.0; W[o] = 0.0; }
         if (h < H) {
             const MwEntry e = ent[h];
 #pragma unroll
@@ -645,38 +650,48 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
                 W[o] = (double)(int)w * sc;
             }
         }
+#pragma unroll
         for (int p = 0; p < NP; ++p) {
             double v = 0.0;
             if (h < H) {
                 double others = 1.0;
+#pragma unroll
                 for (int o = 0; o < NP; ++o) if (o != p) others *= W[o];
-                if (nd.type == MTT_NODE_FOLD) {
-                    const int w = __ffs(am) - 1;
-                    v = (p == w ? (double)nd.pot - (double)nd.c[p] : -(double)d.bf[p * NP + w] * (double)nd.c[p]) * others;
+                const double cp = (double)nd.c[p];
+                if (fold) {
+                    v = (p == winner ? pot - cp : -(double)d.bf[p * NP + winner] * cp) * others;
                 } else if (!((am >> p) & 1)) {
-                    v = -(double)d.bf[p * NP + p] * (double)nd.c[p] * others;
+                    v = -(double)d.bf[p * NP + p] * cp * others;
                 } else {
-                    const double loss = -(double)d.bf[p * NP + p] * (double)nd.c[p];
-                    double inact = 1.0, PW = 1.0, LE = 1.0, Lk[NP - 1], Ek[NP - 1];
-                    int no = 0;
+                    // the opponents in seat order (slots 0..2); an inactive one
+                    // contributes its total mass and never ties
+                    double inact = 1.0, PW = 1.0, LE = 1.0;
+#pragma unroll
                     for (int o = 0; o < NP; ++o) {
                         if (o == p) continue;
-                        if ((am >> o) & 1) {
-                            Lk[no] = L[o]; Ek[no] = E[o];
-                            PW *= W[o];
-                            LE *= L[o] + E[o];
-                            ++no;
-                        } else {
-                            inact *= W[o];
-                        }
+                        if ((am >> o) & 1) { PW *= W[o]; LE *= L[o] + E[o]; }
+                        else inact *= W[o];
                     }
                     double share = 0.0;
-                    for (int T = 0; T < (1 << no); ++T) {
+#pragma unroll
+                    for (int T = 0; T < 8; ++T) {
                         double pr = 1.0;
-                        for (int i = 0; i < no; ++i) pr *= ((T >> i) & 1) ? Ek[i] : Lk[i];
-                        share += pr * ((double)nd.pot / (1 + __popc(T)) - (double)nd.c[p]);
+                        int nt = 0;
+                        bool valid = true;
+                        int slot = 0;
+#pragma unroll
+                        for (int o = 0; o < NP; ++o) {
+                            if (o == p) continue;
+                            const bool act = (am >> o) & 1;
+                            const bool tie = (T >> slot) & 1;
+                            ++slot;
+                            if (!act) { valid = valid && !tie; continue; }
+                            pr *= tie ? E[o] : L[o];
+                            nt += tie ? 1 : 0;
+                        }
+                        if (valid) share += pr * (pot / (1 + nt) - cp);
                     }
-                    v = (share + loss * (PW - LE)) * inact;
+                    v = (share - (double)d.bf[p * NP + p] * cp * (PW - LE)) * inact;
                 }
             }
             outb[(long long)p * Hp + h] = (float)v;
