@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(MT) k_mw_term(MwDev a, const int2* __restrict_
 // and independent of the summation order, so a mass that is zero stays zero.
 // Every prefix is below 3 (2^29 + H / 2) < 2^31; each reach value is off by at
 // most 2^-30 S_o.  The payoffs are then formed in FP64.
-__global__ void __launch_bounds__(MT, 3) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
+__global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restrict__ terms, int n) {
     extern __shared__ __align__(16) int xsi[];       // [NP][3 H + 1] scans, then [NP][Hp] staged reach
     __shared__ int wbi[MT / 32];
     __shared__ float wsum[NP][MT / 32];
