@@ -7,6 +7,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
 
 namespace mtt {
 
@@ -56,6 +57,37 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// Programmatic dependent launch.  A kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may start while the
+// previous kernel on the stream drains; grid_dep_wait returns once that
+// kernel has completed and its writes are visible (immediately when the
+// launch had no such predecessor).  Every such kernel calls it before its
+// first access to data another kernel writes or reads, so completion stays
+// ordered along the stream.  grid_dep_trigger lets the next kernel's CTAs be
+// scheduled once every CTA of this grid has issued it or exited.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launch with programmatic stream serialization when `pdl` (the kernel must
+// call grid_dep_wait before its first dependent access): its CTAs are
+// scheduled while the previous kernel on the stream drains.  Without `pdl`
+// it is an ordinary launch.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                              bool pdl, Args&&... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {

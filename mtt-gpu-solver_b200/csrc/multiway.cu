@@ -38,6 +38,7 @@
 #include <numeric>
 #include <vector>
 
+#include "mtt_bulk.cuh"
 #include "mtt_common.h"
 #include "mtt_device.cuh"
 
@@ -332,7 +333,9 @@ __global__ void __launch_bounds__(256) k_mw_fwd(MwDev a, const MFwd* __restrict_
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
-    const MFwd it = items[w];
+    const MFwd it = items[w];      // work items are written once, before any solve
+    grid_dep_trigger();
+    grid_dep_wait();
     const int g = it.g0 + lane;
     if (g >= it.h4) return;
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -350,7 +353,9 @@ __global__ void __launch_bounds__(256) k_mw_bwd(MwDev a, const MBwd* __restrict_
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= n) return;
-    const MBwd it = items[w];
+    const MBwd it = items[w];      // work items are written once, before any solve
+    grid_dep_trigger();
+    grid_dep_wait();
     const int g = it.g0 + lane;
     if (g >= it.h4) return;
     const int A = it.na, H4 = it.h4, HS4 = it.hs4;
@@ -430,6 +435,8 @@ __global__ void __launch_bounds__(MT) k_mw_term(MwDev a, const int2* __restrict_
     const uint16_t* ge = gs + Hp;
     const long long HS = (long long)NP * Hp;
     const int k_local = node - (int)d.node_base;
+    grid_dep_trigger();
+    grid_dep_wait();
     for (int o = 0; o < NP; ++o) {
         const float* ro = a.arena + d.arena_base + (long long)nd.src[o] * HS + (long long)o * Hp;
         for (int h = tid; h < Hp; h += MT) xs[o * X + (h < H ? pos[h] : h)] = h < H ? (double)ro[h] : 0.0;
@@ -551,6 +558,8 @@ __global__ void __launch_bounds__(MT) k_mw_term_cr(MwDev a, const int2* __restri
     float* rf = reinterpret_cast<float*>(xsi + NP * X);   // [NP][Hp] floats, then the same words as int
     int* ri = xsi + NP * X;
     const int lane = tid & 31, wid = tid >> 5;
+    grid_dep_trigger();
+    grid_dep_wait();
     // stage every player's reach (float4, coalesced) and its absolute mass
     for (int o = 0; o < NP; ++o) {
         const float4* src = reinterpret_cast<const float4*>(a.arena + d.arena_base + (long long)nd.src[o] * HS +
@@ -775,30 +784,42 @@ MwDev mw_args(const mtt_mw_batch* b, int algo, int sem) {
 }
 
 int launch_sweep(const mtt_mw_batch* b, const MwDev& a, int mode, cudaStream_t st) {
+    // every level and the terminals are launched with programmatic stream
+    // serialization (the sweep's first level follows the iteration counter,
+    // an ordinary launch).  A single subgame's launches are short, so the
+    // next kernel's CTAs starting during the previous one's tail pays; the
+    // batched solver chains only within a kernel class.
+    bool chained = false;
     for (int d = 0; d < b->levels; ++d) {
         const long long n = b->fwd_off[d + 1] - b->fwd_off[d];
         if (!n) continue;
         const unsigned grid = (unsigned)((n + 7) / 8);
-        if (mode == MODE_SOLVE) k_mw_fwd<MODE_SOLVE><<<grid, 256, 0, st>>>(a, b->d_fwd + b->fwd_off[d], (int)n);
-        else k_mw_fwd<MODE_AVG><<<grid, 256, 0, st>>>(a, b->d_fwd + b->fwd_off[d], (int)n);
+        const MFwd* items = b->d_fwd + b->fwd_off[d];
+        if (mode == MODE_SOLVE) MTT_TRY_CUDA(launch_pdl(k_mw_fwd<MODE_SOLVE>, grid, 256, 0, st, chained, a, items, (int)n));
+        else MTT_TRY_CUDA(launch_pdl(k_mw_fwd<MODE_AVG>, grid, 256, 0, st, chained, a, items, (int)n));
         MTT_CHECK_LAUNCH();
+        chained = true;
     }
     if (b->n_terms) {
         if (a.semantics == MTT_SEM_CORRECT) {
-            k_mw_term_cr<<<b->n_terms, MT, term_cr_smem(b), st>>>(a, b->d_terms, b->n_terms);
+            MTT_TRY_CUDA(launch_pdl(k_mw_term_cr, (unsigned)b->n_terms, MT, term_cr_smem(b), st, true, a,
+                                    (const int2*)b->d_terms, b->n_terms));
         } else {
             const size_t smem = sizeof(double) * (size_t)NP * ((size_t)b->Hmax + 1);
-            k_mw_term<<<b->n_terms, MT, smem, st>>>(a, b->d_terms, b->n_terms);
+            MTT_TRY_CUDA(launch_pdl(k_mw_term, (unsigned)b->n_terms, MT, smem, st, true, a, (const int2*)b->d_terms, b->n_terms));
         }
         MTT_CHECK_LAUNCH();
     }
+    chained = true;
     for (int d = b->levels - 1; d >= 0; --d) {
         const long long n = b->bwd_off[d + 1] - b->bwd_off[d];
         if (!n) continue;
         const unsigned grid = (unsigned)((n + 7) / 8);
-        if (mode == MODE_SOLVE) k_mw_bwd<MODE_SOLVE><<<grid, 256, 0, st>>>(a, b->d_bwd + b->bwd_off[d], (int)n);
-        else k_mw_bwd<MODE_AVG><<<grid, 256, 0, st>>>(a, b->d_bwd + b->bwd_off[d], (int)n);
+        const MBwd* items = b->d_bwd + b->bwd_off[d];
+        if (mode == MODE_SOLVE) MTT_TRY_CUDA(launch_pdl(k_mw_bwd<MODE_SOLVE>, grid, 256, 0, st, chained, a, items, (int)n));
+        else MTT_TRY_CUDA(launch_pdl(k_mw_bwd<MODE_AVG>, grid, 256, 0, st, chained, a, items, (int)n));
         MTT_CHECK_LAUNCH();
+        chained = true;
     }
     return MTT_OK;
 }

@@ -706,7 +706,9 @@ template <int SPAN>
 __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= n) return;
-    const FwdItem it = items[w];
+    const FwdItem it = items[w];      // work items are written once, before any solve
+    grid_dep_trigger();
+    grid_dep_wait();
 #pragma unroll
     for (int s = 0; s < SPAN; ++s) {
         if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
@@ -811,8 +813,12 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
             bulk_g2s(T, a.tabs + g.tab + tab_idx_off(o, g.H0), ib, &bar[0]);
             bulk_g2s(T + ib, a.tabs + g.tab + tab_ent_off(q1, g.H0, g.H1), tb - ib, &bar[0]);
         }
-        issue_reach(0, 0);
     }
+    // tables and items are written once, before any solve; reach and values
+    // belong to the previous kernels
+    grid_dep_trigger();
+    grid_dep_wait();
+    if (tid == 0) issue_reach(0, 0);
     const bool okt = mbar_wait_bounded(&bar[0], 0u);
     if (__syncthreads_or(!okt)) {
         if (tid == 0) atomicOr(a.err, 1);
@@ -1018,7 +1024,9 @@ template <int SPAN>
 __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= n) return;
-    const BwdItem it = items[w];
+    const BwdItem it = items[w];      // work items are written once, before any solve
+    grid_dep_trigger();
+    grid_dep_wait();
 #pragma unroll
     for (int s = 0; s < SPAN; ++s) {
         if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
@@ -1893,16 +1901,28 @@ static SolveDev dev_args(const mtt_batch* b, const mtt_solve_params& p) {
 
 static int term_xstride(const mtt_batch* b) { return term_scratch(b->max_h); }
 
+// Launches after the first of a kernel class (forward levels, terminal
+// groups, backward levels) are chained with programmatic stream
+// serialization: their CTAs are scheduled during the previous launch's tail
+// and read their work items before grid_dep_wait.  The first launch of each
+// class is ordinary.  Chaining across classes as well measured 5% slower per
+// iteration on the 4,096-subgame batch (backward CTAs then start on SMs still
+// set up for the terminal kernel's shared memory); chaining within classes
+// measured 0.3% faster.
 static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelLists<FwdItem>& L, int threads,
                              cudaStream_t st) {
     const long long warps = threads / 32;
+    bool chained = false;
     for (int d = 0; d < b->levels; ++d) {
         const long long n = L.off[d + 1] - L.off[d];
         if (n == 0) continue;
-        if (a.span == 2) k_fwd<2><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
-        else k_fwd<1><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        if (a.span == 2) MTT_TRY_CUDA(launch_pdl(k_fwd<2>, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
+                                        (const FwdItem*)(L.d + L.off[d]), (int)n));
+        else MTT_TRY_CUDA(launch_pdl(k_fwd<1>, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
+                                        (const FwdItem*)(L.d + L.off[d]), (int)n));
         MTT_CHECK_LAUNCH();
         ++b->launches;
+        chained = true;
     }
     return MTT_OK;
 }
@@ -1910,24 +1930,32 @@ static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelL
 static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelLists<BwdItem>& L, int threads,
                              cudaStream_t st) {
     const long long warps = threads / 32;
+    bool chained = false;
     for (int d = b->levels - 1; d >= 0; --d) {
         const long long n = L.off[d + 1] - L.off[d];
         if (n == 0) continue;
-        if (a.span == 2) k_bwd<2><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
-        else k_bwd<1><<<(unsigned)((n + warps - 1) / warps), threads, 0, st>>>(a, L.d + L.off[d], (int)n);
+        if (a.span == 2) MTT_TRY_CUDA(launch_pdl(k_bwd<2>, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
+                                        (const BwdItem*)(L.d + L.off[d]), (int)n));
+        else MTT_TRY_CUDA(launch_pdl(k_bwd<1>, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
+                                        (const BwdItem*)(L.d + L.off[d]), (int)n));
         MTT_CHECK_LAUNCH();
         ++b->launches;
+        chained = true;
     }
     return MTT_OK;
 }
 
 static int launch_term(const mtt_batch* b, const ListSet& L, const SolveDev& a, int upd, cudaStream_t st) {
+    bool chained = false;
     for (size_t k = 0; k < L.tb_start.size(); ++k) {
         if (L.tb_count[k] == 0) continue;
         const int smem = upd == 3 ? L.tb_smem3[k] : L.tb_smem1[k];
-        k_term<<<L.tb_count[k], TG, smem, st>>>(a, L.tgroups + L.tb_start[k], L.titems, L.tb_count[k], upd);
+        MTT_TRY_CUDA(launch_pdl(k_term, (unsigned)L.tb_count[k], TG, smem, st, chained, a,
+                                (const TermGroup*)(L.tgroups + L.tb_start[k]), (const TermItem*)L.titems,
+                                L.tb_count[k], upd));
         MTT_CHECK_LAUNCH();
         ++b->launches;
+        chained = true;
     }
     return MTT_OK;
 }
