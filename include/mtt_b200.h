@@ -365,6 +365,18 @@ int mtt_batch_destroy(mtt_batch* b);
 int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, void* d_C, int32_t ldc,
                   int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
                   int32_t flags, int32_t* d_err, void* stream);
+/* The same with a caller-owned FP32 workspace of ws_floats floats on the
+ * stream's device.  A product of fewer output tiles (128 x 256) than about
+ * the SM count over at least 512 of K is split along K so that the splits
+ * fill the SMs: each split writes its partial tile to d_ws, and a second
+ * kernel adds the splits in a fixed order and applies the epilogue.  The
+ * split count is lowered until splits x M x N fits ws_floats; with none left
+ * (or d_ws null) it is mtt_gemm_bf16.  Results are deterministic; they
+ * differ from the one-pass kernel's in FP32 summation order only.  d_ws must
+ * not be used by anything else until the call's work on the stream is done. */
+int mtt_gemm_bf16_ws(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, void* d_C, int32_t ldc,
+                     int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
+                     int32_t flags, int32_t* d_err, float* d_ws, int64_t ws_floats, void* stream);
 
 /* ------------------------------------------------------ leaf network */
 /* MLP for depth-limited solving (no reference counterpart): features

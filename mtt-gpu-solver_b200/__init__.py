@@ -151,10 +151,13 @@ def board_showdown_counts(board, hands, stream=None):
 GEMM_RELU, GEMM_OUT_BF16, GEMM_MASK = 1, 2, 4
 
 
-def gemm_bf16(A, B, bias=None, relu=False, out_bf16=False, mask=None, out=None, err=None, stream=None):
+def gemm_bf16(A, B, bias=None, relu=False, out_bf16=False, mask=None, out=None, err=None, stream=None,
+              workspace=None):
     """C = A @ B.T (+ bias, ReLU / ReLU-mask) on the tcgen05 tensor cores.
     A: bf16 CUDA [M, K], B: bf16 CUDA [N, K] (row-major, K contiguous, row
-    strides multiples of 8); C: float32 or bf16 [M, N]."""
+    strides multiples of 8); C: float32 or bf16 [M, N].  workspace: an
+    optional float32 CUDA tensor that lets a product of few output tiles be
+    split along K (mtt_gemm_bf16_ws)."""
     import torch
     M, K = A.shape
     N = B.shape[0]
@@ -167,12 +170,18 @@ def gemm_bf16(A, B, bias=None, relu=False, out_bf16=False, mask=None, out=None, 
     for t in (A, B):
         if t.dtype != torch.bfloat16 or not t.is_cuda or t.stride(1) != 1:
             raise TypeError("A and B must be bf16 CUDA matrices with unit column stride")
-    check("mtt_gemm_bf16", lib().mtt_gemm_bf16(
-        ctypes.c_void_p(A.data_ptr()), A.stride(0), ctypes.c_void_p(B.data_ptr()), B.stride(0),
-        ctypes.c_void_p(out.data_ptr()), out.stride(0), M, N, K,
-        _dev(bias, torch.float32) if bias is not None else None,
-        ctypes.c_void_p(mask.data_ptr()) if mask is not None else None, mask.stride(0) if mask is not None else 0,
-        flags, ctypes.c_void_p(err.data_ptr()), _stream(stream)))
+    args = (ctypes.c_void_p(A.data_ptr()), A.stride(0), ctypes.c_void_p(B.data_ptr()), B.stride(0),
+            ctypes.c_void_p(out.data_ptr()), out.stride(0), M, N, K,
+            _dev(bias, torch.float32) if bias is not None else None,
+            ctypes.c_void_p(mask.data_ptr()) if mask is not None else None, mask.stride(0) if mask is not None else 0,
+            flags, ctypes.c_void_p(err.data_ptr()))
+    if workspace is None:
+        check("mtt_gemm_bf16", lib().mtt_gemm_bf16(*args, _stream(stream)))
+    else:
+        if workspace.dtype != torch.float32 or not workspace.is_cuda or not workspace.is_contiguous():
+            raise TypeError("workspace must be a contiguous float32 CUDA tensor")
+        check("mtt_gemm_bf16_ws", lib().mtt_gemm_bf16_ws(*args, ctypes.c_void_p(workspace.data_ptr()),
+                                                         workspace.numel(), _stream(stream)))
     if own_err:
         torch.cuda.current_stream().synchronize() if stream is None else None
         if int(err.item()):

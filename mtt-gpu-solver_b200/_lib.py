@@ -126,6 +126,8 @@ def lib():
         "mtt_batch_ev_grad": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "mtt_batch_check": ([vp, vp], ctypes.c_int),
         "mtt_gemm_bf16": ([vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp, i32, i32, vp, vp], ctypes.c_int),
+        "mtt_gemm_bf16_ws": ([vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp, i32, i32, vp, vp, ctypes.c_int64, vp],
+                             ctypes.c_int),
         "mtt_leafnet_create": ([i32, ctypes.c_uint64, i32, vp], ctypes.c_int),
         "mtt_leafnet_forward": ([vp, vp, i32, vp, vp], ctypes.c_int),
         "mtt_leafnet_gradients": ([vp, vp, vp, vp, i32, vp, vp], ctypes.c_int),

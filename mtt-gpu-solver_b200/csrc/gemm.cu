@@ -23,6 +23,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "mtt_bulk.cuh"
@@ -92,7 +93,7 @@ __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.
 __global__ void __launch_bounds__(THREADS, 1)
 k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, void* __restrict__ C,
             int M, int N, int K, int ldc, const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
-            int ldm, int flags, int* __restrict__ err) {
+            int ldm, int flags, int* __restrict__ err, int kps, float* __restrict__ ws) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -102,7 +103,10 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
     int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int KT = (K + BK - 1) / BK;
+    // split z of gridDim.z takes k-tiles [kt0, kt0 + KT); with ws its raw
+    // FP32 partial tile goes to ws + z M N (row stride N) for k_gemm_reduce
+    const int kt0 = (int)blockIdx.z * kps;
+    const int KT = min((K + BK - 1) / BK - kt0, kps);
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(accum, 1);
@@ -133,8 +137,8 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
             }
             uint8_t* st = smem + s * STAGE_BYTES;
             mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(st, &ta, kt * BK, m0, &full[s]);
-            tma_load_2d(st + A_BYTES, &tb, kt * BK, n0, &full[s]);
+            tma_load_2d(st, &ta, (kt0 + kt) * BK, m0, &full[s]);
+            tma_load_2d(st + A_BYTES, &tb, (kt0 + kt) * BK, n0, &full[s]);
         }
         // our own copies have landed before the CTA can leave
         for (int j = (kt > STAGES ? kt - STAGES : 0); j < kt; ++j)
@@ -177,6 +181,17 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
             __syncwarp();
             const int col = n0 + c + lane;
             const bool cin = col < N;
+            if (ws) {   // a split's raw partial sums
+                float* W = ws + (size_t)blockIdx.z * M * N;
+#pragma unroll 4
+                for (int i = 0; i < 32; ++i) {
+                    const int row = r0 + i;
+                    if (row >= M) break;
+                    if (cin) W[(size_t)row * N + col] = P[i * 33 + lane];
+                }
+                __syncwarp();
+                continue;
+            }
             const float b = (bias && cin) ? bias[col] : 0.0f;
 #pragma unroll 4
             for (int i = 0; i < 32; ++i) {
@@ -201,6 +216,23 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
+}
+
+// Sum of the splits' partial tiles in split order, then the epilogue of the
+// single-pass kernel (bias, ReLU, ReLU mask, BF16 or FP32 store).
+__global__ void __launch_bounds__(256) k_gemm_reduce(const float* __restrict__ ws, int splits, void* __restrict__ C,
+                                                     int M, int N, int ldc, const float* __restrict__ bias,
+                                                     const __nv_bfloat16* __restrict__ mask, int ldm, int flags) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)M * N) return;
+    const int row = (int)(i / N), col = (int)(i % N);
+    float v = ws[i];
+    for (int z = 1; z < splits; ++z) v += ws[(size_t)z * M * N + i];
+    if (bias) v += bias[col];
+    if ((flags & F_RELU) && v < 0.0f) v = 0.0f;
+    if ((flags & F_MASK) && !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f)) v = 0.0f;
+    if (flags & F_OUT_BF16) reinterpret_cast<__nv_bfloat16*>(C)[(size_t)row * ldc + col] = __float2bfloat16_rn(v);
+    else reinterpret_cast<float*>(C)[(size_t)row * ldc + col] = v;
 }
 
 // Host: the driver's tensor-map encoder, found once through the runtime.
@@ -252,8 +284,26 @@ static int smem_attr_once() {
     return MTT_OK;
 }
 
+// Split-K: a grid of fewer tiles than about the SM count, over at least 8
+// k-tiles of 64, is cut along K into splits of at least 4 k-tiles, so that
+// tiles x splits comes near the SM count; each split writes its partial tile
+// to ws and k_gemm_reduce adds them in split order.  Without ws (or with too
+// small a ws) the GEMM runs in one pass.
+static int choose_splits(int M, int N, int K, size_t ws_floats, int* kps) {
+    const int tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM);
+    const int KT = (K + BK - 1) / BK;
+    *kps = KT;
+    if (!ws_floats || tiles >= 100 || KT < 8) return 1;
+    int splits = std::min(std::max(148 / tiles, 1), KT / 4);
+    while (splits > 1 && (size_t)splits * M * N > ws_floats) --splits;
+    if (splits <= 1) return 1;
+    *kps = (KT + splits - 1) / splits;
+    return (KT + *kps - 1) / *kps;
+}
+
 static int launch(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
-                  const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st) {
+                  const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st,
+                  float* ws, size_t ws_floats) {
     if (M <= 0 || N <= 0 || K <= 0) return M == 0 || N == 0 ? MTT_OK : MTT_ERR_INVALID;
     if (!A || !B || !C || !d_err || (lda % 8) || (ldb % 8) || lda < K || ldb < K || ldc < N) return MTT_ERR_INVALID;
     if (((uintptr_t)A & 15) || ((uintptr_t)B & 15)) return MTT_ERR_INVALID;
@@ -262,18 +312,29 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     MTT_TRY(make_map(&ta, A, M, K, lda, BM));
     MTT_TRY(make_map(&tb, B, N, K, ldb, BN));
     MTT_TRY(smem_attr_once());
-    const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    int kps = 0;
+    const int splits = choose_splits(M, N, K, ws_floats, &kps);
+    const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM), (unsigned)splits);
     k_gemm_bf16<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, C, M, N, K, ldc, bias,
-                                                    reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err);
+                                                    reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err,
+                                                    kps, splits > 1 ? ws : nullptr);
     MTT_CHECK_LAUNCH();
+    if (splits > 1) {
+        const long long n = (long long)M * N;
+        k_gemm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ws, splits, C, M, N, ldc, bias,
+                                                                   reinterpret_cast<const __nv_bfloat16*>(mask), ldm,
+                                                                   flags);
+        MTT_CHECK_LAUNCH();
+    }
     return MTT_OK;
 }
 
 }  // namespace gemm
 
 int gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
-              const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st) {
-    return gemm::launch(A, lda, B, ldb, C, ldc, M, N, K, bias, mask, ldm, flags, d_err, st);
+              const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st, float* ws,
+              size_t ws_floats) {
+    return gemm::launch(A, lda, B, ldb, C, ldc, M, N, K, bias, mask, ldm, flags, d_err, st, ws, ws_floats);
 }
 
 }  // namespace mtt
@@ -282,5 +343,13 @@ extern "C" int mtt_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int3
                              int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
                              int32_t flags, int32_t* d_err, void* stream) {
     return mtt::gemm_bf16(d_A, lda, d_B, ldb, d_C, ldc, M, N, K, d_bias, d_mask, ldm, flags, d_err,
-                          mtt::as_stream(stream));
+                          mtt::as_stream(stream), nullptr, 0);
+}
+
+extern "C" int mtt_gemm_bf16_ws(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, void* d_C, int32_t ldc,
+                                int32_t M, int32_t N, int32_t K, const float* d_bias, const void* d_mask, int32_t ldm,
+                                int32_t flags, int32_t* d_err, float* d_ws, int64_t ws_floats, void* stream) {
+    if (ws_floats < 0 || (ws_floats > 0 && !d_ws)) return MTT_ERR_INVALID;
+    return mtt::gemm_bf16(d_A, lda, d_B, ldb, d_C, ldc, M, N, K, d_bias, d_mask, ldm, flags, d_err,
+                          mtt::as_stream(stream), d_ws, d_ws ? (size_t)ws_floats : 0);
 }

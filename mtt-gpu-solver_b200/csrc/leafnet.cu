@@ -24,7 +24,8 @@
 
 namespace mtt {
 int gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
-              const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st);
+              const float* bias, const void* mask, int ldm, int flags, int* d_err, cudaStream_t st, float* ws,
+              size_t ws_floats);
 
 namespace leaf {
 
@@ -87,13 +88,29 @@ __global__ void k_mse(const float* __restrict__ Y, const float* __restrict__ T, 
     if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
 }
 
-// db[c] = sum over rows of dY[r][c] (fixed order: one thread per column).
-__global__ void k_colsum(const bf16* __restrict__ dY, int M, int N, int ld, float* __restrict__ db) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= N) return;
+// db[c] = sum over rows of dY[r][c], in a fixed order: a CTA of 32 x 32
+// threads takes 32 columns; thread (x, y) sums rows y, y + 32, ... of column
+// x (each warp reads 64 consecutive bytes of a row), then the 32 partial sums
+// of a column are added in slice order.
+constexpr int CS_COLS = 32, CS_SLICES = 32;
+__global__ void __launch_bounds__(CS_COLS * CS_SLICES) k_colsum(const bf16* __restrict__ dY, int M, int N, int ld,
+                                                               float* __restrict__ db) {
+    __shared__ float part[CS_SLICES][CS_COLS + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int c = blockIdx.x * CS_COLS + tx;
     float acc = 0.0f;
-    for (int r = 0; r < M; ++r) acc += __bfloat162float(dY[(size_t)r * ld + c]);
-    db[c] = acc;
+    if (c < N) {
+#pragma unroll 8
+        for (int r = ty; r < M; r += CS_SLICES) acc += __bfloat162float(dY[(size_t)r * ld + c]);
+    }
+    part[ty][tx] = acc;
+    __syncthreads();
+    if (ty == 0 && c < N) {
+        float t = 0.0f;
+#pragma unroll
+        for (int k = 0; k < CS_SLICES; ++k) t += part[k][tx];
+        db[c] = t;
+    }
 }
 
 // Adam on FP32 masters; refreshes the BF16 copy W [rows][cols] (and, in a
@@ -150,11 +167,13 @@ struct mtt_leafnet {
     float* Y = nullptr;
     double* partial = nullptr;
     int* err = nullptr;
+    float* ws = nullptr;                     // split-K partial tiles of the GEMMs with few output tiles
     long long step = 0;
 };
 
 namespace {
 constexpr int MSE_BLOCKS = 592;
+constexpr size_t WS_FLOATS = 8u << 20;      // 32 MB: four 1,024 x 1,024 splits, or ten of 240 x 2,688
 
 template <typename T>
 int dmalloc(T** p, size_t n) {
@@ -168,7 +187,7 @@ void free_net(mtt_leafnet* n) {
         cudaFree(l.gw); cudaFree(l.gb); cudaFree(l.wb); cudaFree(l.wt); cudaFree(l.live);
     }
     cudaFree(n->X0); cudaFree(n->dY); cudaFree(n->T1); cudaFree(n->T2); cudaFree(n->Y); cudaFree(n->partial);
-    cudaFree(n->err);
+    cudaFree(n->err); cudaFree(n->ws);
     for (int k = 0; k < 3; ++k) { cudaFree(n->H[k]); cudaFree(n->dH[k]); }
     delete n;
 }
@@ -204,10 +223,11 @@ int forward(mtt_leafnet* n, const float* d_x, int M, cudaStream_t st) {
     const bf16* in = n->X0;
     for (int l = 0; l < 3; ++l) {
         MTT_TRY(gemm_bf16(in, DIN[l], n->L[l].wb, DIN[l], n->H[l], HID, M, HID, DIN[l], n->L[l].b, nullptr, 0,
-                          F_RELU | F_OUT_BF16, n->err, st));
+                          F_RELU | F_OUT_BF16, n->err, st, n->ws, WS_FLOATS));
         in = n->H[l];
     }
-    return gemm_bf16(in, HID, n->L[3].wb, HID, n->Y, OUTP, M, OUTP, HID, n->L[3].b, nullptr, 0, 0, n->err, st);
+    return gemm_bf16(in, HID, n->L[3].wb, HID, n->Y, OUTP, M, OUTP, HID, n->L[3].b, nullptr, 0, 0, n->err, st, n->ws,
+                     WS_FLOATS);
 }
 
 // Gradients of the masked MSE into L[l].gw / gb; *h_loss = the loss.
@@ -223,14 +243,15 @@ int backward(mtt_leafnet* n, const float* d_y, const float* d_w, int M, double n
         // dW = g^T * act: A = g^T [out][M], B = act^T [in][M]
         MTT_TRY(transpose(g, M, gw, gw, n->T1, M, st));
         MTT_TRY(transpose(acts[l], M, DIN[l], DIN[l], n->T2, M, st));
-        MTT_TRY(gemm_bf16(n->T1, M, n->T2, M, L.gw, L.in, L.out, L.in, M, nullptr, nullptr, 0, 0, n->err, st));
-        k_colsum<<<(unsigned)((L.out + 127) / 128), 128, 0, st>>>(g, M, L.out, gw, L.gb);
+        MTT_TRY(gemm_bf16(n->T1, M, n->T2, M, L.gw, L.in, L.out, L.in, M, nullptr, nullptr, 0, 0, n->err, st, n->ws,
+                          WS_FLOATS));
+        k_colsum<<<(unsigned)((L.out + CS_COLS - 1) / CS_COLS), dim3(CS_COLS, CS_SLICES), 0, st>>>(g, M, L.out, gw, L.gb);
         MTT_CHECK_LAUNCH();
         if (l == 0) break;
         // dH_{l-1} = (g * W) masked by H_{l-1} > 0: A = g [M][out], B = W^T [in][out]
         bf16* dh = n->dH[l - 1];
         MTT_TRY(gemm_bf16(g, gw, L.wt, L.out, dh, HID, M, HID, L.out, nullptr, acts[l], HID, F_MASK | F_OUT_BF16,
-                          n->err, st));
+                          n->err, st, n->ws, WS_FLOATS));
         g = dh;
         gw = HID;
     }
@@ -307,6 +328,7 @@ extern "C" int mtt_leafnet_create(int32_t batch_cap, uint64_t seed, int32_t flag
     if (!s) s = dmalloc(&n->Y, M * OUTP);
     if (!s) s = dmalloc(&n->partial, MSE_BLOCKS);
     if (!s) s = dmalloc(&n->err, 1);
+    if (!s) s = dmalloc(&n->ws, WS_FLOATS);
     if (!s) s = cuda_status(cudaMemset(n->err, 0, sizeof(int)));
     for (int l = 0; l < NL && !s; ++l) s = refresh_bf16(n, l, nullptr);
     if (!s) s = cuda_status(cudaDeviceSynchronize());

@@ -1190,37 +1190,44 @@ __global__ void __launch_bounds__(TG) k_leaf_showdown(SolveDev a, const LeafItem
 
 // Leaf values of the updated players `upd` from the check-down values SD
 // and/or the network output Y with the masses M (either source may be null).
-__global__ void __launch_bounds__(256) k_leaf_values(SolveDev a, const LeafItem* __restrict__ leaves,
-                                                     const float* __restrict__ SD, int sd_stride,
-                                                     const float* __restrict__ Y, const float* __restrict__ M, int upd,
-                                                     float div) {
+// One CTA per (leaf, 128 hands); each hand adds its 48 rivers in card order.
+constexpr int LV_HANDS = 128;
+__global__ void __launch_bounds__(LV_HANDS) k_leaf_values(SolveDev a, const LeafItem* __restrict__ leaves,
+                                                          const float* __restrict__ SD, int sd_stride,
+                                                          const float* __restrict__ Y, const float* __restrict__ M,
+                                                          int upd, float div) {
     __shared__ int rc[LEAF_RIVERS];
+    __shared__ float wm[2][LEAF_RIVERS];        // pot x the opponent's reach mass per river row
     const int tid = threadIdx.x;
     const LeafItem L = leaves[blockIdx.x];
-    if (tid < LEAF_RIVERS) rc[tid] = leaf_river_card(L.board, tid);
+    const int h = blockIdx.y * LV_HANDS + tid;
+    if (tid < LEAF_RIVERS) {
+        rc[tid] = leaf_river_card(L.board, tid);
+        if (Y) {
+            const size_t row = (size_t)L.row0 + tid;
+            wm[0][tid] = __fmul_rn(L.pot, M[2 * row + 1]);   // q = 0 meets player 1's mass
+            wm[1][tid] = __fmul_rn(L.pot, M[2 * row]);
+        }
+    }
     __syncthreads();
     for (int q = 0; q < 2; ++q) {
-        if (!((upd >> q) & 1)) continue;
-        const int o = 1 - q;
-        float* out = a.arena + L.cfv[q];
-        const uint16_t* hc = a.hcards + L.hc[q];
-        for (int h = tid; h < L.Hp[q]; h += 256) {
-            float v = 0.0f;
-            if (h < L.H[q]) {
-                const int cc = hc[h], c1 = cc & 0xFF, c2 = cc >> 8;
-                const int id = q * LEAF_COMBOS + combo_index(c1, c2);
-                float acc = 0.0f;
-                for (int j = 0; j < LEAF_RIVERS; ++j) {
-                    if (rc[j] == c1 || rc[j] == c2) continue;
-                    const size_t row = (size_t)L.row0 + j;
-                    float y = SD ? SD[(row * 2 + q) * sd_stride + h] : 0.0f;
-                    if (Y) y = fmaf(__fmul_rn(L.pot, M[2 * row + o]), Y[row * LEAF_OUT + id], y);
-                    acc += y;
-                }
-                v = __fdiv_rn(acc, div);
+        if (!((upd >> q) & 1) || h >= L.Hp[q]) continue;
+        float v = 0.0f;
+        if (h < L.H[q]) {
+            const int cc = a.hcards[L.hc[q] + h], c1 = cc & 0xFF, c2 = cc >> 8;
+            const int id = q * LEAF_COMBOS + combo_index(c1, c2);
+            float acc = 0.0f;
+#pragma unroll 8
+            for (int j = 0; j < LEAF_RIVERS; ++j) {
+                if (rc[j] == c1 || rc[j] == c2) continue;
+                const size_t row = (size_t)L.row0 + j;
+                float y = SD ? SD[(row * 2 + q) * sd_stride + h] : 0.0f;
+                if (Y) y = fmaf(wm[q][j], Y[row * LEAF_OUT + id], y);
+                acc += y;
             }
-            out[h] = v;
+            v = __fdiv_rn(acc, div);
         }
+        a.arena[L.cfv[q] + h] = v;
     }
 }
 
@@ -1980,7 +1987,8 @@ static int launch_leaves(const mtt_batch* b, const SolveDev& a, int upd, cudaStr
         ++b->launches;
     }
     const float div = (float)(LEAF_RIVERS - 4 + (a.semantics ? 2 : 0));
-    k_leaf_values<<<b->n_leaves, 256, 0, st>>>(a, b->d_leaves, cd ? b->d_lsd : nullptr, b->leaf_sd_stride,
+    const dim3 lv_grid((unsigned)b->n_leaves, (unsigned)((b->leaf_sd_stride + LV_HANDS - 1) / LV_HANDS));
+    k_leaf_values<<<lv_grid, LV_HANDS, 0, st>>>(a, b->d_leaves, cd ? b->d_lsd : nullptr, b->leaf_sd_stride,
                                                b->net ? b->d_ly : nullptr, b->d_lm, upd, div);
     MTT_CHECK_LAUNCH();
     ++b->launches;

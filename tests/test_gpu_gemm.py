@@ -64,3 +64,36 @@ def test_gemm_strided_operands(mtt, cuda):
     R = _ref(A, B, None, False, None)
     assert float((out[:, :140] - R).abs().max()) <= 1e-5 * math.sqrt(128) * float(R.abs().max()) + 1e-6
     assert float(out[:, 140:].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("M,N,K,relu,out_bf16,masked", [
+    (240, 1024, 2752, True, True, False),     # the leaf network's first layer at 5 leaves x 48 rivers
+    (240, 2688, 1024, False, False, False),   # its output layer
+    (1024, 1024, 4096, False, False, False),  # a weight gradient of the training step
+    (200, 130, 1000, False, False, True),     # ragged edges, a ReLU mask
+])
+def test_split_k_workspace_matches_reference_and_one_pass(mtt, cuda, M, N, K, relu, out_bf16, masked):
+    """mtt_gemm_bf16_ws: few output tiles over a long K are split along K
+    into a workspace and added in split order.  Same tolerance as above
+    against the fp32 reference; deterministic (two calls agree bit for bit);
+    a workspace too small for any split gives the one-pass kernel's bits."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(M + 7 * N + K)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).to(cuda)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).to(cuda)
+    bias = torch.randn(N, generator=g).to(cuda)
+    mask = torch.randn(M, N, generator=g).to(torch.bfloat16).to(cuda) if masked else None
+    ws = torch.empty(16 * M * N, dtype=torch.float32, device=cuda)
+    kw = dict(bias=bias, relu=relu, out_bf16=out_bf16, mask=mask)
+    C1 = mtt.gemm_bf16(A, B, workspace=ws, **kw)
+    C2 = mtt.gemm_bf16(A, B, workspace=ws, **kw)
+    assert torch.equal(C1, C2)
+    R = _ref(A, B, bias, relu, mask)
+    tol = 1e-5 * math.sqrt(K) * float(R.abs().max()) + 1e-6       # FP32 summation order
+    if out_bf16:   # plus one bf16 rounding of the FP32 result
+        assert bool(((C1.float() - R).abs() <= 2 ** -8 * R.abs() + tol).all())
+    else:
+        assert float((C1.float() - R).abs().max()) <= tol
+    one = mtt.gemm_bf16(A, B, **kw)
+    tiny = mtt.gemm_bf16(A, B, workspace=ws[: M * N], **kw)   # room for one split only: no split
+    assert torch.equal(tiny, one)
