@@ -123,6 +123,10 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // launched with programmatic stream serialization: the set-up above ran
+    // while the previous kernel drained; its outputs (A, B, C) are ours now
+    grid_dep_trigger();
+    grid_dep_wait();
 
     if (warp == 0 && lane == 0) {
         // producer: stage s of k-tile kt; the stage is free once the MMAs of
@@ -223,6 +227,8 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
 __global__ void __launch_bounds__(256) k_gemm_reduce(const float* __restrict__ ws, int splits, void* __restrict__ C,
                                                      int M, int N, int ldc, const float* __restrict__ bias,
                                                      const __nv_bfloat16* __restrict__ mask, int ldm, int flags) {
+    grid_dep_wait();   // the splits' partial tiles
+    grid_dep_trigger();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)M * N) return;
     const int row = (int)(i / N), col = (int)(i % N);
@@ -315,15 +321,26 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     int kps = 0;
     const int splits = choose_splits(M, N, K, ws_floats, &kps);
     const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM), (unsigned)splits);
-    k_gemm_bf16<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, C, M, N, K, ldc, bias,
-                                                    reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err,
-                                                    kps, splits > 1 ? ws : nullptr);
+    // both kernels wait in grid_dep_wait before touching global memory, so a
+    // programmatic launch only lets their set-up overlap the previous kernel
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SMEM_BYTES;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MTT_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16, ta, tb, C, M, N, K, ldc, bias,
+                                    reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err, kps,
+                                    splits > 1 ? ws : nullptr));
     MTT_CHECK_LAUNCH();
     if (splits > 1) {
         const long long n = (long long)M * N;
-        k_gemm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ws, splits, C, M, N, ldc, bias,
-                                                                   reinterpret_cast<const __nv_bfloat16*>(mask), ldm,
-                                                                   flags);
+        MTT_TRY_CUDA(launch_pdl(k_gemm_reduce, (unsigned)((n + 255) / 256), 256u, 0, st, true, (const float*)ws, splits,
+                                C, M, N, ldc, bias, reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags));
         MTT_CHECK_LAUNCH();
     }
     return MTT_OK;
