@@ -1634,6 +1634,9 @@ using namespace mtt;
 // ====================================================================== host driver
 struct mtt_batch {
     int n = 0;
+    // the streams this batch's work was issued on, each with an event
+    // recorded after its last call; destroy waits on these, not the device
+    std::vector<std::pair<cudaStream_t, cudaEvent_t>> used;
     SubDesc* d_desc = nullptr;
     DNode* d_nodes = nullptr;
     uint8_t* d_tabs = nullptr;
@@ -1731,20 +1734,41 @@ static void free_set(ListSet& L) {
     dfree(L.tgroups);
 }
 
+// Waits for the batch's own work (the events of the streams it ran on; its
+// uploads and allocations are synchronous on the legacy stream), not for the
+// whole device: another host thread may be creating the next batch.  The
+// frees are ordered on the legacy stream, after which the pool hands the
+// memory out again.
 static void free_batch(mtt_batch* b) {
     if (!b) return;
-    cudaDeviceSynchronize();
+    for (auto& u : b->used) {
+        cudaEventSynchronize(u.second);
+        cudaEventDestroy(u.second);
+    }
+    b->used.clear();
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     dfree(b->d_desc); dfree(b->d_nodes); dfree(b->d_tabs); dfree(b->d_hcards);
     dfree(b->d_ranges); dfree(b->d_arena); dfree(b->d_R); dfree(b->d_S);
     dfree(b->d_darena); dfree(b->d_results); dfree(b->d_iter);
-    cudaFree(b->d_iter_tab);
+    dfree(b->d_iter_tab);
     dfree(b->d_err);
     dfree(b->d_leaves); dfree(b->d_lx); dfree(b->d_ly); dfree(b->d_lm); dfree(b->d_lsd);
     free_set(b->full);
     free_set(b->act);
-    cudaStreamSynchronize(0);
     delete b;
+}
+
+// Record that work of the batch was issued on st (after the call's last launch).
+static void note_stream(mtt_batch* b, cudaStream_t st) {
+    for (auto& u : b->used)
+        if (u.first == st) { cudaEventRecord(u.second, st); return; }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamSynchronize(st);   // no event: wait here instead
+        return;
+    }
+    cudaEventRecord(e, st);
+    b->used.emplace_back(st, e);
 }
 
 template <typename T>
@@ -1878,8 +1902,9 @@ static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, 
 // host in double exactly as the oracle does.
 static int fill_iter_table(mtt_batch* b, const mtt_solve_params& p, int iters, cudaStream_t st) {
     if (iters > b->iter_cap || !b->d_iter_tab) {
-        if (b->d_iter_tab) { MTT_TRY_CUDA(cudaStreamSynchronize(st)); cudaFree(b->d_iter_tab); b->d_iter_tab = nullptr; }
-        MTT_TRY_CUDA(cudaMalloc(&b->d_iter_tab, sizeof(float) * 4 * (size_t)std::max(iters, 1)));
+        if (b->d_iter_tab) { MTT_TRY_CUDA(cudaStreamSynchronize(st)); dfree(b->d_iter_tab); b->d_iter_tab = nullptr; }
+        long long unused = 0;
+        MTT_TRY(dalloc(&b->d_iter_tab, 4 * (size_t)std::max(iters, 1), unused));
         b->iter_cap = std::max(iters, 1);
         if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }   // captured the old table
     }
@@ -2199,7 +2224,7 @@ static double term_launch_bytes(const ListSet& L, const std::vector<TermGroup>& 
 }
 }  // namespace mtt
 
-extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
+static int mtt_batch_kernel_profile_impl(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
                                         double* h_bytes, void* stream) {
     using namespace mtt;
     if (!b || !h_ms || !h_bytes || iters <= 0) return MTT_ERR_INVALID;
@@ -2276,6 +2301,13 @@ extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* pr
     int err = 0;
     MTT_TRY_CUDA(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     return err ? MTT_ERR_TIMEOUT : MTT_OK;
+}
+
+extern "C" int mtt_batch_kernel_profile(mtt_batch* b, const mtt_solve_params* prm, int32_t iters, double* h_ms,
+                                        double* h_bytes, void* stream) {
+    const int s = mtt_batch_kernel_profile_impl(b, prm, iters, h_ms, h_bytes, stream);
+    if (b) note_stream(b, as_stream(stream));
+    return s;
 }
 
 extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** out) {
@@ -2549,13 +2581,17 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
 extern "C" int mtt_batch_solve(mtt_batch* b, const mtt_solve_params* prm, void* stream) {
     if (!b) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
-    return run_solve(b, *prm, as_stream(stream), false);
+    const int s = run_solve(b, *prm, as_stream(stream), false);
+    note_stream(b, as_stream(stream));
+    return s;
 }
 
 extern "C" int mtt_batch_solve_graph(mtt_batch* b, const mtt_solve_params* prm, void* stream) {
     if (!b) return MTT_ERR_INVALID;
     MTT_TRY(check_params(prm));
-    return run_solve(b, *prm, as_stream(stream), true);
+    const int s = run_solve(b, *prm, as_stream(stream), true);
+    note_stream(b, as_stream(stream));
+    return s;
 }
 
 extern "C" int mtt_batch_results(mtt_batch* b, double* h_out, void* stream) {
@@ -2698,7 +2734,7 @@ extern "C" int mtt_batch_set_leafnet(mtt_batch* b, mtt_leafnet* net, int32_t fla
     return MTT_OK;
 }
 
-extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
+static int mtt_batch_ev_grad_impl(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
                                  float* d_grad_ranges, float* d_grad_logits, void* stream) {
     auto al16 = [](const void* p) { return p && ((uintptr_t)p & 15u) == 0; };
     if (!b || !al16(d_logits) || !al16(d_ranges) || !d_ev || !al16(d_grad_ranges) || !al16(d_grad_logits))
@@ -2739,6 +2775,13 @@ extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const floa
     MTT_CHECK_LAUNCH();
     ++b->launches;
     return MTT_OK;
+}
+
+extern "C" int mtt_batch_ev_grad(mtt_batch* b, const float* d_logits, const float* d_ranges, float* d_ev,
+                                 float* d_grad_ranges, float* d_grad_logits, void* stream) {
+    const int s = mtt_batch_ev_grad_impl(b, d_logits, d_ranges, d_ev, d_grad_ranges, d_grad_logits, stream);
+    if (b) note_stream(b, as_stream(stream));
+    return s;
 }
 
 extern "C" int mtt_batch_check(mtt_batch* b, void* stream) {
@@ -2790,7 +2833,7 @@ extern "C" int mtt_batch_schedule(mtt_batch* b, int32_t* threads, int32_t* hands
     return MTT_OK;
 }
 
-extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads) {
+static int mtt_batch_autotune_impl(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads) {
     using namespace mtt;
     if (!b) return MTT_ERR_INVALID;
     if (b->n_leaves && !b->leaf_ready) return MTT_ERR_INVALID;
@@ -2833,9 +2876,14 @@ extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, voi
     return MTT_OK;
 }
 
+extern "C" int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, int32_t* threads) {
+    const int s = mtt_batch_autotune_impl(b, prm, stream, threads);
+    if (b) note_stream(b, mtt::as_stream(stream));
+    return s;
+}
+
 extern "C" int mtt_batch_destroy(mtt_batch* b) {
     if (!b) return MTT_ERR_INVALID;
-    cudaDeviceSynchronize();
     free_batch(b);
     return MTT_OK;
 }
