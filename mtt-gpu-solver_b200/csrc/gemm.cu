@@ -2,7 +2,7 @@
 // leaf network: C[M x N] = epilogue(A[M x K] * B[N x K]^T), A and B row-major
 // (K contiguous), FP32 accumulation in tensor memory.
 //
-// One 128 x 256 output tile per CTA of 192 threads:
+// One 128 x 256 output tile per CTA of 576 threads:
 //   warp 0      one thread streams 128 x 64 tiles of A and 256 x 64 of B into a 4-stage
 //               shared-memory ring with 2-D TMA loads (128-byte swizzle),
 //               completing on the stage's "full" mbarrier;
@@ -10,12 +10,13 @@
 //               tcgen05.mma (M=128, N=256, K=16, kind::f16, BF16 in, FP32
 //               accumulate) four times per stage and commits each stage back
 //               to its "empty" mbarrier, then commits the accumulator;
-//   warps 2..5  read the accumulator with tcgen05.ld (warp w owns TMEM lanes
-//               32*(w%4) .. +31 = output rows), 32 columns at a time, and turn
-//               each 32 x 32 block through a padded shared-memory tile (the
-//               operand ring is idle by then) so that each store instruction
-//               writes 32 consecutive columns of one row; add the bias, apply
-//               ReLU or a ReLU mask, convert and store.
+//   warps 2..17 read the accumulator with tcgen05.ld (warp w owns TMEM lanes
+//               32*(w%4) .. +31 = output rows; warps 2-5 take columns 0-63,
+//               6-9 the next 64, and so on), add the bias, apply ReLU or a
+//               ReLU mask, convert, and stage 32-row boxes in the (now idle)
+//               operand ring for TMA stores; an output whose rows are not
+//               16-byte aligned goes through a padded transpose tile instead,
+//               one row of 32 columns per store instruction.
 // Every mbarrier wait is bounded; a wait that gives up sets *err, the
 // producer still waits (bounded) for its own copies and the allocating warp
 // frees the TMEM before the CTA leaves.
@@ -24,6 +25,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "mtt_bulk.cuh"
@@ -32,7 +34,7 @@
 namespace mtt {
 namespace gemm {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, THREADS = 192;
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, THREADS = 576;
 constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // tiles (1024-aligned) + barriers
 constexpr uint32_t TMEM_COLS = BN;   // one FP32 column per output column
@@ -90,10 +92,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// TMA store of one staged box (this CTA's shared memory -> global) through a
+// 3-D map, in this thread's bulk group.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(x),
+                 "r"(y), "r"(z), "r"(smem_addr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Output paths of the epilogue.
+enum { OUT_DIRECT = 0, OUT_TMA_C = 1, OUT_TMA_WS = 2 };
+
 __global__ void __launch_bounds__(THREADS, 1)
-k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, void* __restrict__ C,
+k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+            const __grid_constant__ CUtensorMap tc, int out_mode, void* __restrict__ C,
             int M, int N, int K, int ldc, const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
-            int ldm, int flags, int* __restrict__ err, int kps, float* __restrict__ ws) {
+            int ldm, int flags, int* __restrict__ err, int kps, float* __restrict__ ws, int ldw) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -169,12 +187,86 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
         tc_fence_after();
         if (!ok) atomicOr(err, 1);
         const int lg = warp & 3;                     // TMEM lanes 32*lg .. 32*lg+31
+        const int c_lo = ((warp - 2) >> 2) * (BN / 4), c_hi = c_lo + BN / 4;   // this warp's 64 columns
         const int r0 = m0 + 32 * lg;
         const bool live = ok && !*(volatile int*)s_fail;
+        if (out_mode != OUT_DIRECT) {
+            // Each lane holds one output row.  A box is 32 rows x 128 bytes
+            // (32 FP32 or 64 BF16 columns), staged in the now idle operand
+            // ring with the 128-byte swizzle (16-byte chunk j of row r at
+            // chunk j ^ (r & 7): one store instruction fills 4 banks-wide
+            // wavefronts) and written by one TMA store; two boxes per warp
+            // alternate so that filling one overlaps the other's store.
+            const bool to_bf16 = out_mode == OUT_TMA_C && (flags & F_OUT_BF16);
+            const int groups = to_bf16 ? 2 : 1;                  // 32-column TMEM groups per box
+            uint8_t* stage = smem + (size_t)(warp - 2) * 8192;
+            const int row = r0 + lane;
+            int k = 0;
+#pragma unroll 1
+            for (int c = c_lo; c < c_hi; c += 32 * groups, ++k) {
+                uint8_t* box = stage + (k & 1) * 4096;
+                if (lane == 0) bulk_wait_read_1();                // the store that last read this box is done
+                __syncwarp();
+                bool any = false;
+#pragma unroll 1
+                for (int g = 0; g < groups; ++g) {
+                    const int cg = c + 32 * g;
+                    uint32_t r[32];
+                    tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)cg, r);
+                    tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(cg + 16), r + 16);
+                    tmem_ld_wait();
+                    if (!live || n0 + cg >= N || r0 >= M) continue;   // warp-uniform
+                    any = true;
+                    if (out_mode == OUT_TMA_C) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = n0 + cg + j;
+                            float v = __uint_as_float(r[j]);
+                            if (bias) v += col < N ? __ldg(bias + col) : 0.0f;
+                            if ((flags & F_RELU) && v < 0.0f) v = 0.0f;
+                            if ((flags & F_MASK) && row < M && col < N &&
+                                !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f))
+                                v = 0.0f;
+                            r[j] = __float_as_uint(v);
+                        }
+                    }
+                    if (to_bf16) {   // 32 columns = 64 bytes = chunks 4 g .. 4 g + 3
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            uint32_t w[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const __nv_bfloat162 h = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 2 * e]),
+                                                                               __uint_as_float(r[8 * q + 2 * e + 1]));
+                                w[e] = *reinterpret_cast<const uint32_t*>(&h);
+                            }
+                            const int ch = (4 * g + q) ^ (lane & 7);
+                            *reinterpret_cast<uint4*>(box + lane * 128 + ch * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+                        }
+                    } else {         // 32 columns = 128 bytes = chunks 0 .. 7
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int ch = q ^ (lane & 7);
+                            *reinterpret_cast<uint4*>(box + lane * 128 + ch * 16) =
+                                make_uint4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+                        }
+                    }
+                }
+                if (!any) continue;                                   // warp-uniform
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    tma_store_3d(&tc, box, n0 + c, r0, out_mode == OUT_TMA_WS ? (int)blockIdx.z : 0);
+                    bulk_commit();
+                }
+            }
+            if (lane == 0) bulk_wait_all();
+            __syncwarp();
+        } else {
         // this warp's 32 x 33 transpose tile in the (now idle) operand ring
         float* P = reinterpret_cast<float*>(smem) + (warp - 2) * 32 * 33;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 32) {
+        for (int c = c_lo; c < c_hi; c += 32) {
             uint32_t r[32];
             tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)c, r);
             tmem_ld16(tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(c + 16), r + 16);
@@ -186,12 +278,12 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
             const int col = n0 + c + lane;
             const bool cin = col < N;
             if (ws) {   // a split's raw partial sums
-                float* W = ws + (size_t)blockIdx.z * M * N;
+                float* W = ws + (size_t)blockIdx.z * M * ldw;
 #pragma unroll 4
                 for (int i = 0; i < 32; ++i) {
                     const int row = r0 + i;
                     if (row >= M) break;
-                    if (cin) W[(size_t)row * N + col] = P[i * 33 + lane];
+                    if (cin) W[(size_t)row * ldw + col] = P[i * 33 + lane];
                 }
                 __syncwarp();
                 continue;
@@ -212,6 +304,7 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
             }
             __syncwarp();
         }
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -224,16 +317,18 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
 
 // Sum of the splits' partial tiles in split order, then the epilogue of the
 // single-pass kernel (bias, ReLU, ReLU mask, BF16 or FP32 store).
-__global__ void __launch_bounds__(256) k_gemm_reduce(const float* __restrict__ ws, int splits, void* __restrict__ C,
-                                                     int M, int N, int ldc, const float* __restrict__ bias,
+__global__ void __launch_bounds__(256) k_gemm_reduce(const float* __restrict__ ws, int ldw, int splits,
+                                                     void* __restrict__ C, int M, int N, int ldc,
+                                                     const float* __restrict__ bias,
                                                      const __nv_bfloat16* __restrict__ mask, int ldm, int flags) {
     grid_dep_wait();   // the splits' partial tiles
     grid_dep_trigger();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)M * N) return;
     const int row = (int)(i / N), col = (int)(i % N);
-    float v = ws[i];
-    for (int z = 1; z < splits; ++z) v += ws[(size_t)z * M * N + i];
+    const size_t w = (size_t)row * ldw + col;
+    float v = ws[w];
+    for (int z = 1; z < splits; ++z) v += ws[(size_t)z * M * ldw + w];
     if (bias) v += bias[col];
     if ((flags & F_RELU) && v < 0.0f) v = 0.0f;
     if ((flags & F_MASK) && !(__bfloat162float(mask[(size_t)row * ldm + col]) > 0.0f)) v = 0.0f;
@@ -260,6 +355,22 @@ static int encoder(PFN_cuTensorMapEncodeTiled_v12000* out) {
 
 // 2-D map of a row-major bf16 matrix [rows x cols] with leading dimension ld,
 // box 64 (cols) x box_rows (rows), 128-byte swizzle, zero fill outside.
+// 3-D map of an output [z][rows][cols] with row stride ld elements of esize
+// bytes: boxes of 32 rows x 128 bytes, 128-byte swizzle (the epilogue's
+// staging layout).  ld * esize must be a multiple of 16.
+static int make_out_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, int esize, int rows, int cols, int ld,
+                        int z) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc;
+    MTT_TRY(encoder(&enc));
+    const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)z};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld * esize, (cuuint64_t)rows * ld * esize};
+    const cuuint32_t box[3] = {(cuuint32_t)(128 / esize), 32, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MTT_OK : MTT_ERR_INVALID;
+}
+
 static int make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, int box_rows) {
     PFN_cuTensorMapEncodeTiled_v12000 enc;
     MTT_TRY(encoder(&enc));
@@ -295,13 +406,13 @@ static int smem_attr_once() {
 // tiles x splits comes near the SM count; each split writes its partial tile
 // to ws and k_gemm_reduce adds them in split order.  Without ws (or with too
 // small a ws) the GEMM runs in one pass.
-static int choose_splits(int M, int N, int K, size_t ws_floats, int* kps) {
+static int choose_splits(int M, int N, int K, int ldw, size_t ws_floats, int* kps) {
     const int tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM);
     const int KT = (K + BK - 1) / BK;
     *kps = KT;
     if (!ws_floats || tiles >= 100 || KT < 8) return 1;
     int splits = std::min(std::max(148 / tiles, 1), KT / 4);
-    while (splits > 1 && (size_t)splits * M * N > ws_floats) --splits;
+    while (splits > 1 && (size_t)splits * M * ldw > ws_floats) --splits;
     if (splits <= 1) return 1;
     *kps = (KT + splits - 1) / splits;
     return (KT + *kps - 1) / *kps;
@@ -319,7 +430,25 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     MTT_TRY(make_map(&tb, B, N, K, ldb, BN));
     MTT_TRY(smem_attr_once());
     int kps = 0;
-    const int splits = choose_splits(M, N, K, ws_floats, &kps);
+    const int ldw = (N + 3) & ~3;                  // workspace rows of 16-byte multiples
+    const int splits = choose_splits(M, N, K, ldw, ws_floats, &kps);
+    // the output path: TMA stores of staged boxes when the destination rows
+    // are 16-byte aligned, else per-lane stores
+    CUtensorMap tc;
+    std::memset(&tc, 0, sizeof(tc));
+    int out_mode = OUT_DIRECT;
+    if (splits > 1) {
+        if (!((uintptr_t)ws & 15) &&
+            make_out_map(&tc, ws, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N, ldw, splits) == MTT_OK)
+            out_mode = OUT_TMA_WS;
+    } else {
+        const bool obf = flags & F_OUT_BF16;
+        const int es = obf ? 2 : 4;
+        if (!((uintptr_t)C & 15) && ((size_t)ldc * es) % 16 == 0 &&
+            make_out_map(&tc, C, obf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, es, M, N, ldc,
+                         1) == MTT_OK)
+            out_mode = OUT_TMA_C;
+    }
     const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM), (unsigned)splits);
     // both kernels wait in grid_dep_wait before touching global memory, so a
     // programmatic launch only lets their set-up overlap the previous kernel
@@ -333,14 +462,15 @@ static int launch(const void* A, int lda, const void* B, int ldb, void* C, int l
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    MTT_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16, ta, tb, C, M, N, K, ldc, bias,
+    MTT_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_bf16, ta, tb, tc, out_mode, C, M, N, K, ldc, bias,
                                     reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags, d_err, kps,
-                                    splits > 1 ? ws : nullptr));
+                                    splits > 1 ? ws : nullptr, ldw));
     MTT_CHECK_LAUNCH();
     if (splits > 1) {
         const long long n = (long long)M * N;
-        MTT_TRY_CUDA(launch_pdl(k_gemm_reduce, (unsigned)((n + 255) / 256), 256u, 0, st, true, (const float*)ws, splits,
-                                C, M, N, ldc, bias, reinterpret_cast<const __nv_bfloat16*>(mask), ldm, flags));
+        MTT_TRY_CUDA(launch_pdl(k_gemm_reduce, (unsigned)((n + 255) / 256), 256u, 0, st, true, (const float*)ws, ldw,
+                                splits, C, M, N, ldc, bias, reinterpret_cast<const __nv_bfloat16*>(mask), ldm,
+                                flags));
         MTT_CHECK_LAUNCH();
     }
     return MTT_OK;
