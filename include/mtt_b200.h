@@ -351,6 +351,10 @@ int mtt_batch_autotune(mtt_batch* b, const mtt_solve_params* prm, void* stream, 
  * hands_per_warp 128 or 256, term_chunk 1..16.  Rebuilds the work lists. */
 int mtt_batch_set_schedule(mtt_batch* b, int32_t threads, int32_t hands_per_warp, int32_t term_chunk);
 int mtt_batch_schedule(mtt_batch* b, int32_t* threads, int32_t* hands_per_warp, int32_t* term_chunk);
+/* Waits for the batch's work on the streams it was used with (an event per
+ * stream, recorded by each call that launched work), not for the whole
+ * device, then returns its memory to the pool in legacy-stream order; another
+ * host thread may keep creating or solving other batches meanwhile. */
 int mtt_batch_destroy(mtt_batch* b);
 
 /* ------------------------------------------------------ leaf-net GEMM */
