@@ -288,7 +288,8 @@ def other_configs(mtt, wl, stream):
     # single river subgame, uniform ranges, 1,000 CFR+ iterations + FP64 exploitability
     sub = wl.river_uniform(seed=0)
     b = mtt.RiverBatch([sub])
-    p0 = mtt.solve_params(iters=1000, threads=256, avg_power=2.0)
+    p0 = mtt.solve_params(iters=1000, threads=0, avg_power=2.0)
+    p0.threads = b.autotune(p0)        # the library's schedule search (untimed)
     b.solve(p0, graph=True)
     t = _event_ms(lambda: b.solve(p0, graph=True), stream)
     out["river_single"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
@@ -298,8 +299,9 @@ def other_configs(mtt, wl, stream):
     # turn + river DCFR
     sub = wl.turn_dcfr(seed=1)
     b = mtt.RiverBatch([sub])
-    p1 = mtt.solve_params(iters=500, algo=mtt.ALGO_DCFR, alpha=1.5, beta=0.0, gamma=2.0, threads=256)
-    b.solve(mtt.solve_params(iters=5, algo=mtt.ALGO_DCFR, threads=256), graph=True)
+    p1 = mtt.solve_params(iters=500, algo=mtt.ALGO_DCFR, alpha=1.5, beta=0.0, gamma=2.0, threads=0)
+    p1.threads = b.autotune(p1)
+    b.solve(mtt.solve_params(iters=5, algo=mtt.ALGO_DCFR, threads=p1.threads), graph=True)
     t = _event_ms(lambda: b.solve(p1, graph=True), stream)
     out["turn_river_dcfr"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
                               "nodes": int(len(sub["nodes"])), "iter_bytes": b.info()["iter_bytes"],
@@ -381,6 +383,7 @@ def other_configs(mtt, wl, stream):
     sub = wl.flop_runout(seed=9)
     b = mtt.RiverBatch([sub])
     pf3 = mtt.solve_params(iters=300, alternate=True, avg_power=2.0)
+    pf3.threads = b.autotune(pf3)
     b.solve(pf3, graph=True)
     t = _event_ms(lambda: b.solve(pf3, graph=True), stream)
     out["flop_turn_runout"] = {"ms": t, "exploitability_pct_pot": float(b.results()[0, 5] * 100),
