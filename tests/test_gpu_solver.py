@@ -290,3 +290,31 @@ def test_autotune_picks_a_schedule(mtt, wl, cuda):
     b.solve(p, graph=True)
     assert np.array_equal(r1, b.results())
     b.close()
+
+
+def test_destroy_waits_for_its_own_solve_and_frees_for_the_next_batch(mtt, wl, cuda):
+    """mtt_batch_destroy waits on the streams the batch ran on, not on the
+    device: a batch destroyed right after its solve was queued on a
+    non-blocking stream must not hand its memory to the next batch while the
+    solve still runs.  The next batch (created from the pool right away)
+    solves to the same bits as a batch created on a quiet device."""
+    import torch
+    subs = wl.river_batch(n=64, seed=5, min_support=200, max_support=700)
+    p = mtt.solve_params(iters=30, threads=128)
+    ref = mtt.RiverBatch(subs[32:])
+    ref.solve(p, graph=True)
+    want = ref.results()
+    want_s = ref.read(3)
+    ref.close()
+    side = torch.cuda.Stream()
+    a = mtt.RiverBatch(subs[:32])
+    with torch.cuda.stream(side):
+        a.solve(p, stream=side, graph=True)
+    a.close()                           # no synchronisation by the caller
+    b = mtt.RiverBatch(subs[32:])       # reuses the pool's memory
+    b.solve(p, graph=True)
+    got = b.results()
+    got_s = b.read(3)
+    b.close()
+    assert np.array_equal(want, got)
+    assert np.array_equal(want_s["R0"], got_s["R0"]) and np.array_equal(want_s["S1"], got_s["S1"])
