@@ -23,6 +23,8 @@
 // engine.cu:41-83,219-257) and the DCFR weights of kernel_dcfr_step
 // (preflop_grid_generator.cu:387-410, in the discount-then-add form).
 #include <algorithm>
+#include <atomic>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -2514,19 +2516,32 @@ extern "C" int mtt_batch_create(const mtt_subgame* subs, int32_t n, mtt_batch** 
         dst.reserve(k);
         for (int t = 0; t < nlt; ++t) dst.insert(dst.end(), get(part[t]).begin(), get(part[t]).end());
     };
+    // every list is merged by its own job (distinct vectors), the jobs on the
+    // host threads
+    std::vector<std::function<void()>> jobs;
+    auto add = [&](auto get) { jobs.emplace_back([&merge, get]() { merge(get); }); };
     for (int d = 0; d < levels; ++d) {
-        merge([d](HostLists& L) -> std::vector<Task>& { return L.bf[d]; });
-        merge([d](HostLists& L) -> std::vector<Task>& { return L.bb[d]; });
-        merge([d](HostLists& L) -> std::vector<FwdItem>& { return L.fi[d]; });
-        merge([d](HostLists& L) -> std::vector<FwdItem>& { return L.fsim[d]; });
-        merge([d](HostLists& L) -> std::vector<BwdItem>& { return L.bsim[d]; });
+        add([d](HostLists& L) -> std::vector<Task>& { return L.bf[d]; });
+        add([d](HostLists& L) -> std::vector<Task>& { return L.bb[d]; });
+        add([d](HostLists& L) -> std::vector<FwdItem>& { return L.fi[d]; });
+        add([d](HostLists& L) -> std::vector<FwdItem>& { return L.fsim[d]; });
+        add([d](HostLists& L) -> std::vector<BwdItem>& { return L.bsim[d]; });
         for (int u = 0; u < 2; ++u) {
-            merge([d, u](HostLists& L) -> std::vector<FwdItem>& { return L.fal[u][d]; });
-            merge([d, u](HostLists& L) -> std::vector<BwdItem>& { return L.bal[u][d]; });
+            add([d, u](HostLists& L) -> std::vector<FwdItem>& { return L.fal[u][d]; });
+            add([d, u](HostLists& L) -> std::vector<BwdItem>& { return L.bal[u][d]; });
         }
     }
-    merge([](HostLists& L) -> std::vector<TermItem>& { return L.titems; });
-    merge([](HostLists& L) -> std::vector<int2>& { return L.terms; });
+    add([](HostLists& L) -> std::vector<TermItem>& { return L.titems; });
+    add([](HostLists& L) -> std::vector<int2>& { return L.terms; });
+    {
+        std::atomic<size_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < nlt; ++t)
+            th.emplace_back([&]() {
+                for (size_t j; (j = next.fetch_add(1)) < jobs.size();) jobs[j]();
+            });
+        for (auto& x : th) x.join();
+    }
     for (int t = 0; t < nlt; ++t) b->h_leaves.insert(b->h_leaves.end(), plv[t].begin(), plv[t].end());
     for (size_t k = 0; k < b->h_leaves.size(); ++k) b->h_leaves[k].row0 = LEAF_RIVERS * (int)k;
     long long total = 0;
