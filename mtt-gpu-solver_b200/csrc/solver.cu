@@ -635,7 +635,7 @@ __device__ __forceinline__ void bwd_sum_fixed(const float4* __restrict__ qc, flo
 
 // Forward sweep of one level: regret matching, children's reach and/or
 // strategy sums (kernel_forward_sweep, honest_multistreet_solver.cu:88-126).
-template <int ALGO>
+template <int ALGO, bool SUMS>
 __device__ __forceinline__ void k_fwd_group(const SolveDev& a, const FwdItem& it, const int lane) {
     const float4* rp = reinterpret_cast<const float4*>(a.arena + it.reach_in);
     float4* ch = reinterpret_cast<float4*>(a.arena + it.child);
@@ -659,7 +659,7 @@ __device__ __forceinline__ void k_fwd_group(const SolveDev& a, const FwdItem& it
         }
         return;
     }
-    const bool dr = it.flags & FI_REACH, ds = it.flags & FI_SUMS;
+    const bool dr = it.flags & FI_REACH, ds = SUMS && (it.flags & FI_SUMS);
     const float4* Rb = reinterpret_cast<const float4*>(a.R + it.rows);
     float4* Sb = reinterpret_cast<float4*>(a.S + it.rows);
     if (dr && !ds) {
@@ -705,8 +705,11 @@ __device__ __forceinline__ void k_fwd_group(const SolveDev& a, const FwdItem& it
 }
 
 // One warp per work item; the item covers span x 32 float4 hand groups.
-// ALGO: the solve's a.algo.
-template <int SPAN, int ALGO>
+// ALGO: the solve's a.algo; SUMS: the list may hold FI_SUMS items (without
+// it, such items would pass reach only).  The reach-only kernel of the
+// alternating passes took 0.734 ms per iteration on the 4,096-subgame river
+// batch against 0.771 ms for the kernel that also handles strategy sums.
+template <int SPAN, int ALGO, bool SUMS>
 __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= n) return;
@@ -716,7 +719,7 @@ __global__ void __launch_bounds__(256, 5) k_fwd(SolveDev a, const FwdItem* __res
 #pragma unroll
     for (int s = 0; s < SPAN; ++s) {
         if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
-        k_fwd_group<ALGO>(a, it, (threadIdx.x & 31) + 32 * s);
+        k_fwd_group<ALGO, SUMS>(a, it, (threadIdx.x & 31) + 32 * s);
     }
 }
 
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(TG, 5) k_term(SolveDev a, const TermGroup* __r
 
 // Backward sweep of one level for the updated players: counterfactual values
 // and the CFR+/DCFR regret update (kernel_backward_sweep, honest:198-249).
-template <int ALGO>
+template <int ALGO, bool SUMS>
 __device__ __forceinline__ void k_bwd_group(const SolveDev& a, const BwdItem& it, const int lane) {
     const float4* qc = reinterpret_cast<const float4*>(a.arena + it.child);
     float4* out = reinterpret_cast<float4*>(a.arena + it.self);
@@ -983,7 +986,7 @@ __device__ __forceinline__ void k_bwd_group(const SolveDev& a, const BwdItem& it
     float4* Rb = reinterpret_cast<float4*>(a.R + it.rows);
     float dpos = 0.f, dneg = 0.f, w_lin = 0.f, dstr = 0.f;
     constexpr bool dcfr = ALGO == MTT_ALGO_DCFR;
-    const bool ds = it.flags & BI_SUMS;
+    const bool ds = SUMS && (it.flags & BI_SUMS);
     for (int k = 0; k < A; ++k) {
         pf_l2(qc + (size_t)k * HS4 + g);
         if (ds) pf_l2(reinterpret_cast<const float4*>(a.S + it.rows) + (size_t)k * H4 + g);
@@ -1042,8 +1045,9 @@ __device__ __forceinline__ void k_bwd_group(const SolveDev& a, const BwdItem& it
 // ALGO: the solve's a.algo (a kernel per algorithm: on the 4,096-subgame
 // river batch the backward levels took 1.87 ms per iteration against 1.91 ms
 // with the update rule chosen at run time; 64 registers a thread at four CTAs
-// per SM, without the spills, took 1.94 ms).
-template <int SPAN, int ALGO>
+// per SM, without the spills, took 1.94 ms).  SUMS: the list may hold
+// BI_SUMS items (without it, such items would update regrets only).
+template <int SPAN, int ALGO, bool SUMS>
 __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __restrict__ items, int n) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= n) return;
@@ -1053,7 +1057,7 @@ __global__ void __launch_bounds__(256, 5) k_bwd(SolveDev a, const BwdItem* __res
 #pragma unroll
     for (int s = 0; s < SPAN; ++s) {
         if (SPAN > 1 && it.g0 + 32 * s >= it.h4) break;
-        k_bwd_group<ALGO>(a, it, (threadIdx.x & 31) + 32 * s);
+        k_bwd_group<ALGO, SUMS>(a, it, (threadIdx.x & 31) + 32 * s);
     }
 }
 
@@ -1964,8 +1968,10 @@ static int term_xstride(const mtt_batch* b) { return term_scratch(b->max_h); }
 // iteration on the 4,096-subgame batch (backward CTAs then start on SMs still
 // set up for the terminal kernel's shared memory); chaining within classes
 // measured 0.3% faster.
+// sums: the lists add to the strategy sums (simultaneous-update forward
+// lists, alternating-update backward lists).
 static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelLists<FwdItem>& L, int threads,
-                             cudaStream_t st) {
+                             bool sums, cudaStream_t st) {
     const long long warps = threads / 32;
     bool chained = false;
     for (int d = 0; d < b->levels; ++d) {
@@ -1973,8 +1979,13 @@ static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelL
         if (n == 0) continue;
         using K = void (*)(SolveDev, const FwdItem*, int);
         const bool dc = a.algo == MTT_ALGO_DCFR;
-        const K k = a.span == 2 ? (dc ? k_fwd<2, MTT_ALGO_DCFR> : k_fwd<2, MTT_ALGO_CFRPLUS>)
-                                : (dc ? k_fwd<1, MTT_ALGO_DCFR> : k_fwd<1, MTT_ALGO_CFRPLUS>);
+        // reach-only lists do not depend on the update rule
+        const K k = a.span == 2 ? (!sums ? k_fwd<2, MTT_ALGO_CFRPLUS, false>
+                                   : dc  ? k_fwd<2, MTT_ALGO_DCFR, true>
+                                         : k_fwd<2, MTT_ALGO_CFRPLUS, true>)
+                                : (!sums ? k_fwd<1, MTT_ALGO_CFRPLUS, false>
+                                   : dc  ? k_fwd<1, MTT_ALGO_DCFR, true>
+                                         : k_fwd<1, MTT_ALGO_CFRPLUS, true>);
         MTT_TRY_CUDA(launch_pdl(k, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
                                 (const FwdItem*)(L.d + L.off[d]), (int)n));
         MTT_CHECK_LAUNCH();
@@ -1985,7 +1996,7 @@ static int launch_levels_fwd(const mtt_batch* b, const SolveDev& a, const LevelL
 }
 
 static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelLists<BwdItem>& L, int threads,
-                             cudaStream_t st) {
+                             bool sums, cudaStream_t st) {
     const long long warps = threads / 32;
     bool chained = false;
     for (int d = b->levels - 1; d >= 0; --d) {
@@ -1993,8 +2004,12 @@ static int launch_levels_bwd(const mtt_batch* b, const SolveDev& a, const LevelL
         if (n == 0) continue;
         using K = void (*)(SolveDev, const BwdItem*, int);
         const bool dc = a.algo == MTT_ALGO_DCFR;
-        const K k = a.span == 2 ? (dc ? k_bwd<2, MTT_ALGO_DCFR> : k_bwd<2, MTT_ALGO_CFRPLUS>)
-                                : (dc ? k_bwd<1, MTT_ALGO_DCFR> : k_bwd<1, MTT_ALGO_CFRPLUS>);
+        static const K ks[2][2][2] = {   // [span - 1][dcfr][sums]
+            {{k_bwd<1, MTT_ALGO_CFRPLUS, false>, k_bwd<1, MTT_ALGO_CFRPLUS, true>},
+             {k_bwd<1, MTT_ALGO_DCFR, false>, k_bwd<1, MTT_ALGO_DCFR, true>}},
+            {{k_bwd<2, MTT_ALGO_CFRPLUS, false>, k_bwd<2, MTT_ALGO_CFRPLUS, true>},
+             {k_bwd<2, MTT_ALGO_DCFR, false>, k_bwd<2, MTT_ALGO_DCFR, true>}}};
+        const K k = ks[a.span == 2 ? 1 : 0][dc ? 1 : 0][sums ? 1 : 0];
         MTT_TRY_CUDA(launch_pdl(k, (unsigned)((n + warps - 1) / warps), threads, 0, st, chained, a,
                                 (const BwdItem*)(L.d + L.off[d]), (int)n));
         MTT_CHECK_LAUNCH();
@@ -2060,16 +2075,16 @@ static int launch_iteration(const mtt_batch* b, const ListSet& L, const SolveDev
                             int threads, cudaStream_t st) {
     if (p.alternate) {
         for (int u = 0; u < 2; ++u) {
-            MTT_TRY(launch_levels_fwd(b, a, L.f_alt[u], threads, st));
+            MTT_TRY(launch_levels_fwd(b, a, L.f_alt[u], threads, false, st));
             MTT_TRY(launch_leaves(b, a, 1 << u, st));
             MTT_TRY(launch_term(b, L, a, 1 << u, st));
-            MTT_TRY(launch_levels_bwd(b, a, L.b_alt[u], threads, st));
+            MTT_TRY(launch_levels_bwd(b, a, L.b_alt[u], threads, true, st));
         }
     } else {
-        MTT_TRY(launch_levels_fwd(b, a, L.f_sim, threads, st));
+        MTT_TRY(launch_levels_fwd(b, a, L.f_sim, threads, true, st));
         MTT_TRY(launch_leaves(b, a, 3, st));
         MTT_TRY(launch_term(b, L, a, 3, st));
-        MTT_TRY(launch_levels_bwd(b, a, L.b_sim, threads, st));
+        MTT_TRY(launch_levels_bwd(b, a, L.b_sim, threads, false, st));
     }
     k_next_iter<<<1, 32, 0, st>>>(a);
     MTT_CHECK_LAUNCH();
@@ -2203,7 +2218,7 @@ static int run_solve(mtt_batch* b, const mtt_solve_params& p, cudaStream_t st, b
     k_init<<<b->n, 256, 0, st>>>(a, b->n);
     MTT_CHECK_LAUNCH();
     ++b->launches;
-    MTT_TRY(launch_levels_fwd(b, a, b->full.f_init, threads, st));
+    MTT_TRY(launch_levels_fwd(b, a, b->full.f_init, threads, false, st));
     MTT_TRY(run_iterations(b, b->full, a, p, threads, p.iters, graph, true, st));
     std::fill(b->iters_done.begin(), b->iters_done.end(), p.iters);
     if (p.exploitability) MTT_TRY(launch_br(b, b->full, a, threads, st));
@@ -2298,7 +2313,7 @@ static int mtt_batch_kernel_profile_impl(mtt_batch* b, const mtt_solve_params* p
     k_init<<<b->n, 256, 0, st>>>(a, b->n);
     MTT_CHECK_LAUNCH();
     ++b->launches;
-    MTT_TRY(launch_levels_fwd(b, a, L.f_init, threads, st));
+    MTT_TRY(launch_levels_fwd(b, a, L.f_init, threads, false, st));
     // one event before and after each kernel class of every pass
     const int passes = p.alternate ? 2 : 1, ne = 6 * passes;
     std::vector<cudaEvent_t> ev(ne, nullptr);
@@ -2311,13 +2326,13 @@ static int mtt_batch_kernel_profile_impl(mtt_batch* b, const mtt_solve_params* p
             const LevelLists<FwdItem>& F = p.alternate ? L.f_alt[u] : L.f_sim;
             const LevelLists<BwdItem>& B = p.alternate ? L.b_alt[u] : L.b_sim;
             s = cuda_status(cudaEventRecord(e[0], st));
-            if (!s) s = launch_levels_fwd(b, a, F, threads, st);
+            if (!s) s = launch_levels_fwd(b, a, F, threads, !p.alternate, st);
             if (!s) s = cuda_status(cudaEventRecord(e[1], st));
             if (!s) s = cuda_status(cudaEventRecord(e[2], st));
             if (!s) s = launch_term(b, L, a, p.alternate ? 1 << u : 3, st);
             if (!s) s = cuda_status(cudaEventRecord(e[3], st));
             if (!s) s = cuda_status(cudaEventRecord(e[4], st));
-            if (!s) s = launch_levels_bwd(b, a, B, threads, st);
+            if (!s) s = launch_levels_bwd(b, a, B, threads, p.alternate != 0, st);
             if (!s) s = cuda_status(cudaEventRecord(e[5], st));
         }
         if (!s) {
