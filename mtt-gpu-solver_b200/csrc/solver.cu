@@ -1896,12 +1896,26 @@ static int build_set(mtt_batch* b, ListSet& L, const std::vector<char>* active, 
     }
     // Buckets: ascending hand count, three equal-count launches whose shared
     // memory is sized by their largest group; inside a bucket the costliest
-    // groups go first so that the last wave is made of short ones.
+    // groups go first so that the last wave is made of short ones.  Groups
+    // that all fit in one wave at the largest group's shared memory (a single
+    // subgame, the few still above the exploitability gate) take one launch:
+    // the buckets' launches run one after another, each as long as its
+    // slowest CTA.
     std::stable_sort(gr.begin(), gr.end(), [](const TermGroup& x, const TermGroup& y) {
         return std::max(x.Hp0, x.Hp1) < std::max(y.Hp0, y.Hp1);
     });
     L.tb_start.clear(); L.tb_count.clear(); L.tb_smem1.clear(); L.tb_smem3.clear();
-    const int ng = (int)gr.size(), nb = ng < 3 ? 1 : 3;
+    int all1 = 0, all3 = 0;
+    for (const TermGroup& g : gr) {
+        all1 = std::max(all1, std::max(tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 1),
+                                       tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 2)));
+        all3 = std::max(all3, tg_smem_bytes(g.H0, g.H1, g.Hp0, g.Hp1, 3));
+    }
+    // CTAs per SM at a dynamic shared-memory size: 228 KB per SM, 4 KB a CTA
+    // for its static shared memory and the system's reserve, 5 at most (registers)
+    auto per_sm = [](int dyn) { return std::max(1, std::min(5, (228 * 1024) / (dyn + 4 * 1024))); };
+    const long long wave = (long long)std::min(per_sm(all1), per_sm(all3)) * std::max(sm_count, 1);
+    const int ng = (int)gr.size(), nb = ng < 3 || ng <= wave ? 1 : 3;
     for (int k = 0; k < nb; ++k) {
         const int lo = (int)((long long)ng * k / nb), hi = (int)((long long)ng * (k + 1) / nb);
         std::stable_sort(gr.begin() + lo, gr.begin() + hi, [](const TermGroup& x, const TermGroup& y) {
